@@ -1,0 +1,24 @@
+"""apspie_b200: B200-native (sm_100a) SpMSpV / hash-SpGEMM graph hot path.
+
+The product is the C-ABI shared library built from ``apspie_b200/csrc`` (declared in
+``include/apspie.h``); this package loads it with ctypes for tests and benchmarks.
+"""
+from ._lib import ApspieError, ApspieLibraryMissing, LIB_PATH, VAL_F32, VAL_I32, VAL_NONE, lib
+from .graph import (
+    Context,
+    DeviceGraph,
+    HostGraph,
+    gen_er,
+    gen_rmat,
+    lcc_sample,
+    load_mtx,
+    max_degree_vertex,
+    mt19937_u32,
+    strict_lower,
+)
+
+__all__ = [
+    "ApspieError", "ApspieLibraryMissing", "LIB_PATH", "VAL_F32", "VAL_I32", "VAL_NONE", "lib",
+    "Context", "DeviceGraph", "HostGraph", "gen_er", "gen_rmat", "lcc_sample", "load_mtx",
+    "max_degree_vertex", "mt19937_u32", "strict_lower",
+]

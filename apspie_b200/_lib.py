@@ -1,0 +1,128 @@
+"""ctypes binding of the in-tree C-ABI library ``apspie_b200/lib/libapspie.so``.
+
+The library is the product; this module only describes its structs and signatures
+(``include/apspie.h``, ``include/apspie_host.h``) and turns status codes into exceptions.
+There is no fallback: if the shared library is missing, importing the entry points
+raises ``ApspieLibraryMissing``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_uint32, c_void_p
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libapspie.so")
+
+STATUS = {
+    0: "APSPIE_OK",
+    1: "APSPIE_ERR_INVALID_ARG",
+    2: "APSPIE_ERR_OOM",
+    3: "APSPIE_ERR_HASH_OVERFLOW",
+    4: "APSPIE_ERR_TIMEOUT",
+    5: "APSPIE_ERR_CUDA",
+    6: "APSPIE_ERR_UNSUPPORTED",
+    7: "APSPIE_ERR_NOT_CONVERGED",
+}
+VAL_NONE, VAL_F32, VAL_I32 = 0, 1, 2
+
+
+class ApspieLibraryMissing(RuntimeError):
+    pass
+
+
+class ApspieError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+
+
+class CSR(ctypes.Structure):
+    _fields_ = [
+        ("m", c_int32), ("n", c_int32), ("nnz", c_int32), ("val_type", c_int32),
+        ("row_ptr", c_void_p), ("col_ind", c_void_p), ("val", c_void_p),
+    ]
+
+
+class CSROwned(ctypes.Structure):
+    _fields_ = [
+        ("m", c_int32), ("n", c_int32), ("nnz", c_int32), ("val_type", c_int32),
+        ("row_ptr", c_void_p), ("col_ind", c_void_p), ("val", c_void_p),
+    ]
+
+
+class HostCSR(ctypes.Structure):
+    _fields_ = [
+        ("m", c_int32), ("n", c_int32), ("nnz", c_int32), ("val_type", c_int32),
+        ("row_ptr", POINTER(c_int32)), ("col_ind", POINTER(c_int32)), ("val", c_void_p),
+    ]
+
+
+class RunStats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", c_int32), ("push_iterations", c_int32), ("pull_iterations", c_int32),
+        ("reserved", c_int32), ("edges_expanded", c_int64), ("edges_component", c_int64),
+        ("vertices_reached", c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    # context
+    "apspie_ctx_create": (c_int, [c_int, c_void_p, POINTER(c_void_p)]),
+    "apspie_ctx_destroy": (None, [c_void_p]),
+    "apspie_ctx_last_error": (c_char_p, [c_void_p]),
+    "apspie_ctx_synchronize": (c_int, [c_void_p]),
+    "apspie_ctx_reserve": (c_int, [c_void_p, c_int32, c_int64]),
+    "apspie_ctx_set_validate": (c_int, [c_void_p, c_int]),
+    "apspie_ctx_set_bfs_tuning": (c_int, [c_void_p, c_float, c_float]),
+    "apspie_ctx_scratch_bytes": (c_int64, [c_void_p]),
+    "apspie_csr_validate": (c_int, [c_void_p, POINTER(CSR)]),
+    # traversal
+    "apspie_bfs": (c_int, [c_void_p, POINTER(CSR), c_int32, c_int32, c_void_p, POINTER(RunStats)]),
+    "apspie_sssp": (c_int, [c_void_p, POINTER(CSR), c_int32, c_void_p, POINTER(RunStats)]),
+    "apspie_mis": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p, POINTER(RunStats)]),
+    "apspie_spmspv_bool": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p]),
+    # host graph construction
+    "apspie_host_csr_free": (None, [POINTER(HostCSR)]),
+    "apspie_load_mtx": (c_int, [c_char_p, c_int, POINTER(HostCSR)]),
+    "apspie_gen_rmat": (c_int, [c_int, c_int, c_uint32, c_uint32, c_double, c_double, c_double,
+                                c_int, POINTER(HostCSR)]),
+    "apspie_gen_er": (c_int, [c_int, c_int, c_uint32, c_int, POINTER(HostCSR)]),
+    "apspie_mt19937_u32": (c_int, [c_uint32, c_int64, c_void_p]),
+    "apspie_max_degree_vertex": (c_int32, [POINTER(HostCSR)]),
+    "apspie_lcc_sample": (c_int, [POINTER(HostCSR), c_int32, c_uint32, c_void_p]),
+    "apspie_csr_strict_lower": (c_int, [POINTER(HostCSR), POINTER(HostCSR)]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads (once) and returns the shared library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ApspieLibraryMissing(
+                f"{LIB_PATH} not found: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                "or `make -C apspie_b200/csrc`")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(status: int, ctx=None, what: str = "") -> None:
+    if status != 0:
+        msg = what
+        if ctx is not None:
+            raw = lib().apspie_ctx_last_error(ctx)
+            if raw:
+                msg = f"{what}: {raw.decode(errors='replace')}"
+        raise ApspieError(status, msg)

@@ -1,0 +1,211 @@
+// Shared device/host plumbing for the apspie B200 kernels: the context object, the
+// scratch arena, the bounded grid barrier used by the persistent traversal kernels, and
+// block-wide scan helpers. sm_100a only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/apspie.h"
+
+namespace apspie {
+
+// ---------------------------------------------------------------------------------
+// Per-call device control block. Reset by the host (one memset) before each launch.
+// ---------------------------------------------------------------------------------
+struct TravCtl {
+    unsigned bar_count;  // grid barrier arrival counter
+    unsigned bar_gen;    // grid barrier generation
+    int err;             // first apspie_status error raised on the device
+    int err_where;       // kernel-defined location code of that error
+    int qlen[2];         // frontier queue lengths (ping-pong)
+    int iterations;
+    int push_iterations;
+    int pull_iterations;
+    int pad0;
+    long long edges_expanded;
+    long long edges_component;
+    long long vertices_reached;
+    long long aux[4];    // kernel-specific counters
+};
+
+// Upper bound on a persistent grid (chunk sums are staged in shared memory).
+constexpr int kMaxGrid = 2048;
+// A grid barrier gives up after this long (ns) and raises APSPIE_ERR_TIMEOUT.
+constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;
+
+}  // namespace apspie
+
+struct apspie_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 0;
+    std::string last_error;
+    // scratch arena: one device allocation, carved per call, grown on demand
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    // control block (device) + pinned host mirror
+    apspie::TravCtl *d_ctl = nullptr;
+    apspie::TravCtl *h_ctl = nullptr;
+    int *d_sticky_err = nullptr;  // errors of asynchronous calls, read by synchronize
+    int *h_word = nullptr;        // pinned scratch word for small device->host reads
+    int validate = 0;
+    float bfs_alpha = 14.0f;
+    float bfs_beta = 24.0f;
+};
+
+namespace apspie {
+
+// ---------------------------------------------------------------------------------
+// Host helpers
+// ---------------------------------------------------------------------------------
+apspie_status set_error(apspie_ctx *ctx, apspie_status st, const std::string &msg);
+apspie_status cuda_error(apspie_ctx *ctx, cudaError_t e, const char *what);
+// Ensures the arena holds `bytes`; returns its base in *out.
+apspie_status scratch_reserve(apspie_ctx *ctx, size_t bytes, void **out);
+// Validates a CSR view on the device (synchronises). Used when ctx->validate is on.
+apspie_status validate_csr(apspie_ctx *ctx, const apspie_csr *A, bool need_square);
+// Checks host-visible CSR view fields (no device access).
+apspie_status check_csr_view(apspie_ctx *ctx, const apspie_csr *A, const char *who);
+// Cooperative launch of a persistent kernel with the largest co-resident grid.
+apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, void **args,
+                                int *grid_out, int max_grid = kMaxGrid);
+// Copies the control block back, synchronises, and turns a device error into a status.
+apspie_status finish_call(apspie_ctx *ctx, apspie_run_stats *stats, const char *who);
+
+// Carves aligned sub-buffers out of the scratch arena.
+struct Carver {
+    char *base;
+    size_t off = 0;
+    explicit Carver(void *b) : base(static_cast<char *>(b)) {}
+    template <typename T>
+    T *take(size_t count) {
+        off = (off + 255) & ~size_t(255);
+        T *p = reinterpret_cast<T *>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+    static size_t need(std::initializer_list<size_t> sizes) {
+        size_t o = 0;
+        for (size_t s : sizes) o = ((o + 255) & ~size_t(255)) + s;
+        return o + 256;
+    }
+};
+
+// ---------------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------------
+#ifdef __CUDACC__
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ int ld_volatile_i32(const int *p) {
+    return *reinterpret_cast<const volatile int *>(p);
+}
+
+__device__ __forceinline__ void raise_error(TravCtl *ctl, int *sticky, int status, int where) {
+    if (atomicCAS(&ctl->err, 0, status) == 0) ctl->err_where = where;
+    atomicCAS(sticky, 0, status);
+}
+
+// Grid-wide barrier for a cooperatively launched (co-resident) grid. Every wait is
+// bounded by kBarrierTimeoutNs; on timeout it raises APSPIE_ERR_TIMEOUT and returns
+// false, as it does whenever any block has raised an error, so that all blocks leave
+// the persistent loop together instead of hanging.
+__device__ __forceinline__ bool grid_barrier(TravCtl *ctl, int *sticky, int where) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned nblocks = gridDim.x;
+        unsigned gen = ld_acquire_u32(&ctl->bar_gen);
+        __threadfence();
+        unsigned prev = atomicAdd(&ctl->bar_count, 1u);
+        if (prev == nblocks - 1) {
+            ctl->bar_count = 0;
+            __threadfence();
+            st_release_u32(&ctl->bar_gen, gen + 1);
+        } else {
+            unsigned long long t0 = globaltimer_ns();
+            while (ld_acquire_u32(&ctl->bar_gen) == gen) {
+                if (ld_volatile_i32(&ctl->err) != 0) { ok = 0; break; }
+                __nanosleep(100);
+                if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+                    raise_error(ctl, sticky, APSPIE_ERR_TIMEOUT, where);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        if (ld_volatile_i32(&ctl->err) != 0) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Block-wide exclusive scan of one int per thread. `tmp` must hold 33 ints.
+template <int BLOCK>
+__device__ __forceinline__ int block_exclusive_scan(int x, int &total, int *tmp) {
+    static_assert(BLOCK % 32 == 0 && BLOCK <= 1024, "block size");
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) tmp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int w = lane < NW ? tmp[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < NW) tmp[lane] = wi - w;  // exclusive warp base
+        if (lane == NW - 1) tmp[32] = wi;   // block total
+    }
+    __syncthreads();
+    int res = tmp[wid] + incl - x;
+    total = tmp[32];
+    __syncthreads();
+    return res;
+}
+
+// Warp-aggregated append of `v` to queue `q` for lanes with pred set. All 32 lanes of
+// the warp must call it.
+__device__ __forceinline__ void warp_append(bool pred, int v, int *q, int *qlen) {
+    unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (mask == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(qlen, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) q[base + __popc(mask & ((1u << lane) - 1u))] = v;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace apspie

@@ -1,0 +1,643 @@
+// Persistent SpMSpV traversal kernels: BFS (boolean OR-AND), SSSP (min-plus), MIS
+// (priority max), and the one-hop boolean SpMSpV.
+//
+// Each algorithm is ONE cooperative launch whose blocks loop over levels/iterations with
+// a bounded grid barrier between phases; the host never reads a count mid-run. This
+// replaces the reference's host-driven level loops (src/bfs.cuh:87-110,
+// src/spmspvBfs.cuh:174-222, src/sssp.cuh:79-98, src/spmspvMis.cuh:232-318), which issue
+// ~10-14 launches, up to 3 device->host syncs and a cudaMalloc/cudaFree per level, and
+// which stop after a caller-supplied `depth` taken from the CPU BFS.
+#include <cstdio>
+
+#include "frontier.cuh"
+
+namespace apspie {
+
+namespace {
+
+constexpr int kBlock = 512;
+constexpr int kVT = 4;
+using Smem = ExpandSmem<kBlock, kVT>;
+
+constexpr int kInf = 0x7fffffff;
+
+// device error sites (reported as err_where)
+enum : int {
+    kSiteBfs = 100,
+    kSiteSssp = 200,
+    kSiteSsspNegWeight = 201,
+    kSiteSsspOverflow = 202,
+    kSiteSsspIterCap = 203,
+    kSiteMis = 300,
+    kSiteMisRoundCap = 301,
+};
+
+struct TravBuffers {
+    int *q0, *q1, *rs, *loc_off, *chunk_sum, *aux;
+    unsigned *bits0, *bits1, *bits2;
+};
+
+size_t trav_scratch_bytes(int m) {
+    const size_t words = (static_cast<size_t>(m) + 31) / 32;
+    const size_t mi = static_cast<size_t>(m) + 1;
+    return Carver::need({mi * 4, mi * 4, mi * 4, mi * 4, kMaxGrid * 4, mi * 4, words * 4,
+                         words * 4, words * 4});
+}
+
+TravBuffers carve_trav(void *base, int m) {
+    const size_t words = (static_cast<size_t>(m) + 31) / 32;
+    const size_t mi = static_cast<size_t>(m) + 1;
+    Carver c(base);
+    TravBuffers b;
+    b.q0 = c.take<int>(mi);
+    b.q1 = c.take<int>(mi);
+    b.rs = c.take<int>(mi);
+    b.loc_off = c.take<int>(mi);
+    b.chunk_sum = c.take<int>(kMaxGrid);
+    b.aux = c.take<int>(mi);
+    b.bits0 = c.take<unsigned>(words);
+    b.bits1 = c.take<unsigned>(words);
+    b.bits2 = c.take<unsigned>(words);
+    return b;
+}
+
+// ================================================================================
+// BFS
+// ================================================================================
+struct BfsArgs {
+    int m, nnz, src, depth_cap;
+    const int *__restrict__ row_ptr;
+    const int *__restrict__ col_ind;
+    int *depth;
+    TravBuffers buf;  // bits0 = visited, bits1/bits2 = frontier bitmaps (ping-pong)
+    TravCtl *ctl;
+    int *sticky;
+    float alpha, beta;
+};
+
+// Level-synchronous BFS. Level L discovers the vertices at hop distance L.
+//  push (top-down): merge-path expansion of the frontier queue; a neighbour is claimed by
+//      an atomicOr test-and-set on the visited bitmap (the dedup that replaces the
+//      reference's radix sort, src/spmspvBfs.cuh:195-197), its depth written, and it is
+//      appended to the next queue by a warp-aggregated ballot.
+//  pull (bottom-up): one warp per 32-vertex bitmap word; each unvisited vertex scans its
+//      row until it meets a frontier vertex (frontier bitmap built in phase A).
+// The direction follows Beamer's rule on the edges out of the frontier (m_f) against the
+// edges still unexplored (m_u): push->pull when m_f > m_u/alpha, pull->push when the
+// frontier holds fewer than m/beta vertices. Depth results do not depend on the choice.
+__global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
+    __shared__ Smem sm;
+    const int G = gridDim.x;
+    const int gtid = blockIdx.x * kBlock + threadIdx.x;
+    const int gstride = G * kBlock;
+    const int m = a.m;
+    const int words = (m + 31) >> 5;
+    unsigned *vis = a.buf.bits0;
+
+    for (int i = gtid; i < m; i += gstride) a.depth[i] = (i == a.src) ? 0 : -1;
+    for (int w = gtid; w < words; w += gstride) {
+        vis[w] = (w == (a.src >> 5)) ? (1u << (a.src & 31)) : 0u;
+        a.buf.bits1[w] = 0u;
+        a.buf.bits2[w] = 0u;
+    }
+    if (gtid == 0) {
+        a.buf.q0[0] = a.src;
+        a.ctl->qlen[0] = 1;
+        a.ctl->qlen[1] = 0;
+    }
+    if (!grid_barrier(a.ctl, a.sticky, kSiteBfs)) return;
+
+    int cur = 0;
+    bool pull = false;
+    long long visited_edges = 0, reached = 0, expanded = 0;
+    int levels = 0, npush = 0, npull = 0;
+    for (int L = 1;; ++L) {
+        const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
+        if (nf == 0) break;
+        if (a.depth_cap > 0 && L >= a.depth_cap) break;
+        int *qc = cur ? a.buf.q1 : a.buf.q0;
+        int *qn = cur ? a.buf.q0 : a.buf.q1;
+        unsigned *fbc = cur ? a.buf.bits2 : a.buf.bits1;
+        unsigned *fbn = cur ? a.buf.bits1 : a.buf.bits2;
+        int *qlen_next = &a.ctl->qlen[cur ^ 1];
+
+        // phase A: frontier degrees + frontier bitmap
+        frontier_phase_a<kBlock>(qc, nf, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum,
+                                 sm.scan_tmp, [&](int, int v, int deg) {
+                                     atomicOr(fbc + (v >> 5), 1u << (v & 31));
+                                     return deg;
+                                 });
+        if (gtid == 0) *qlen_next = 0;
+        if (!grid_barrier(a.ctl, a.sticky, kSiteBfs + 1)) return;
+
+        const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
+        visited_edges += E;
+        reached += nf;
+        expanded += E;
+        const long long m_u = static_cast<long long>(a.nnz) - visited_edges;
+        if (!pull) {
+            if (a.alpha > 0.0f && static_cast<double>(E) > static_cast<double>(m_u) / a.alpha)
+                pull = true;
+        } else if (static_cast<double>(nf) < static_cast<double>(m) / a.beta) {
+            pull = false;
+        }
+        ++levels;
+
+        // phase B
+        if (!pull) {
+            ++npush;
+            const int *col = a.col_ind;
+            int *depth = a.depth;
+            frontier_expand<kBlock, kVT>(
+                nf, E, a.buf.loc_off, a.buf.rs, sm, [](int, int, Smem &) {},
+                [&](bool valid, int, int idx, Smem &) {
+                    bool fresh = false;
+                    int v = 0;
+                    if (valid) {
+                        v = __ldg(col + idx);
+                        const unsigned bit = 1u << (v & 31);
+                        unsigned *wp = vis + (v >> 5);
+                        if (!(__ldcg(wp) & bit)) {
+                            const unsigned old = atomicOr(wp, bit);
+                            if (!(old & bit)) {
+                                fresh = true;
+                                depth[v] = L;
+                            }
+                        }
+                    }
+                    warp_append(fresh, v, qn, qlen_next);
+                });
+        } else {
+            ++npull;
+            const int lane = threadIdx.x & 31;
+            const int nwarps = gstride >> 5;
+            for (int w = gtid >> 5; w < words; w += nwarps) {
+                const unsigned vw = __ldcg(vis + w);
+                const int v = (w << 5) + lane;
+                bool found = false;
+                if (v < m && !(vw & (1u << lane))) {
+                    const int r0 = __ldg(a.row_ptr + v), r1 = __ldg(a.row_ptr + v + 1);
+                    for (int e = r0; e < r1; ++e) {
+                        const int u = __ldg(a.col_ind + e);
+                        if (__ldcg(fbc + (u >> 5)) & (1u << (u & 31))) {
+                            found = true;
+                            break;
+                        }
+                    }
+                }
+                const unsigned fm = __ballot_sync(0xffffffffu, found);
+                if (fm) {
+                    if (lane == 0) vis[w] = vw | fm;  // this warp owns word w in pull
+                    if (found) a.depth[v] = L;
+                    warp_append(found, v, qn, qlen_next);
+                }
+            }
+        }
+        // the other frontier bitmap is idle this level: clear it for level L+1
+        for (int w = gtid; w < words; w += gstride) fbn[w] = 0u;
+        if (!grid_barrier(a.ctl, a.sticky, kSiteBfs + 2)) return;
+        cur ^= 1;
+    }
+    if (gtid == 0) {
+        a.ctl->iterations = levels;
+        a.ctl->push_iterations = npush;
+        a.ctl->pull_iterations = npull;
+        a.ctl->edges_expanded = expanded;
+        a.ctl->edges_component = visited_edges;
+        a.ctl->vertices_reached = reached;
+    }
+}
+
+// ================================================================================
+// SSSP
+// ================================================================================
+struct SsspArgs {
+    int m, nnz, src;
+    const int *__restrict__ row_ptr;
+    const int *__restrict__ col_ind;
+    const int *__restrict__ w;
+    int *dist;
+    TravBuffers buf;  // bits0 = "queued for next iteration"; aux = distance snapshot
+    TravCtl *ctl;
+    int *sticky;
+};
+
+// Frontier Bellman-Ford with min-plus SpMSpV: the frontier is the set of vertices whose
+// distance dropped in the previous iteration (the reference's dense "every finite entry"
+// frontier, src/spmspvSssp.cuh:31-36, restricted to the changed ones). A relaxation is a
+// plain read of dist[v] and, only if it improves, an atomicMin; the winner of the
+// queued-bit test-and-set appends v to the next queue. The result is the fixed point
+// (exact shortest distances for non-negative integer weights), independent of the order
+// in which relaxations land.
+__global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
+    __shared__ Smem sm;
+    const int G = gridDim.x;
+    const int gtid = blockIdx.x * kBlock + threadIdx.x;
+    const int gstride = G * kBlock;
+    const int m = a.m;
+    const int words = (m + 31) >> 5;
+    unsigned *inq = a.buf.bits0;
+
+    for (int i = gtid; i < m; i += gstride) a.dist[i] = (i == a.src) ? 0 : kInf;
+    for (int w = gtid; w < words; w += gstride) inq[w] = (w == (a.src >> 5)) ? (1u << (a.src & 31)) : 0u;
+    if (gtid == 0) {
+        a.buf.q0[0] = a.src;
+        a.ctl->qlen[0] = 1;
+        a.ctl->qlen[1] = 0;
+    }
+    if (!grid_barrier(a.ctl, a.sticky, kSiteSssp)) return;
+
+    int cur = 0;
+    long long expanded = 0;
+    int iters = 0;
+    for (;;) {
+        const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
+        if (nf == 0) break;
+        if (iters > m + 1) {  // cannot happen with non-negative weights
+            if (gtid == 0) raise_error(a.ctl, a.sticky, APSPIE_ERR_NOT_CONVERGED, kSiteSsspIterCap);
+            break;
+        }
+        int *qc = cur ? a.buf.q1 : a.buf.q0;
+        int *qn = cur ? a.buf.q0 : a.buf.q1;
+        int *qlen_next = &a.ctl->qlen[cur ^ 1];
+        int *snap = a.buf.aux;
+        int *dist = a.dist;
+
+        // phase A: dequeue (clear queued bit), snapshot distance, degrees
+        frontier_phase_a<kBlock>(qc, nf, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum,
+                                 sm.scan_tmp, [&](int i, int v, int deg) {
+                                     atomicAnd(inq + (v >> 5), ~(1u << (v & 31)));
+                                     snap[i] = __ldcg(dist + v);
+                                     return deg;
+                                 });
+        if (gtid == 0) *qlen_next = 0;
+        if (!grid_barrier(a.ctl, a.sticky, kSiteSssp + 1)) return;
+
+        const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
+        expanded += E;
+        ++iters;
+        const int *col = a.col_ind;
+        const int *wt = a.w;
+        TravCtl *ctl = a.ctl;
+        int *sticky = a.sticky;
+        frontier_expand<kBlock, kVT>(
+            nf, E, a.buf.loc_off, a.buf.rs, sm,
+            [&](int j, int k, Smem &s) { s.aux[k] = __ldcg(snap + j); },
+            [&](bool valid, int k, int idx, Smem &s) {
+                bool fresh = false;
+                int v = 0;
+                if (valid) {
+                    v = __ldg(col + idx);
+                    const int we = __ldg(wt + idx);
+                    const long long nd = static_cast<long long>(s.aux[k]) + we;
+                    if (we < 0) {
+                        raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSsspNegWeight);
+                    } else if (nd >= kInf) {
+                        raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSsspOverflow);
+                    } else {
+                        const int ndi = static_cast<int>(nd);
+                        if (ndi < __ldcg(dist + v)) {
+                            const int old = atomicMin(dist + v, ndi);
+                            if (ndi < old) {
+                                const unsigned bit = 1u << (v & 31);
+                                const unsigned ob = atomicOr(inq + (v >> 5), bit);
+                                fresh = !(ob & bit);
+                            }
+                        }
+                    }
+                }
+                warp_append(fresh, v, qn, qlen_next);
+            });
+        if (!grid_barrier(a.ctl, a.sticky, kSiteSssp + 2)) return;
+        cur ^= 1;
+    }
+    // unreached -> -1, and the component statistics
+    long long comp = 0, reached = 0;
+    for (int i = gtid; i < m; i += gstride) {
+        const int d = a.dist[i];
+        if (d == kInf) {
+            a.dist[i] = -1;
+        } else {
+            comp += __ldg(a.row_ptr + i + 1) - __ldg(a.row_ptr + i);
+            ++reached;
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        comp += __shfl_down_sync(0xffffffffu, comp, o);
+        reached += __shfl_down_sync(0xffffffffu, reached, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (comp || reached)) {
+        atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->edges_component),
+                  static_cast<unsigned long long>(comp));
+        atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->vertices_reached),
+                  static_cast<unsigned long long>(reached));
+    }
+    if (gtid == 0) {
+        a.ctl->iterations = iters;
+        a.ctl->push_iterations = iters;
+        a.ctl->edges_expanded = expanded;
+    }
+}
+
+// ================================================================================
+// MIS
+// ================================================================================
+enum : unsigned char { kUndecided = 0, kIn = 1, kOut = 2 };
+
+struct MisArgs {
+    int m, nnz;
+    const int *__restrict__ row_ptr;
+    const int *__restrict__ col_ind;
+    const unsigned *__restrict__ prio;
+    unsigned char *member;
+    unsigned char *state;
+    int *blocked;  // round stamp: "an undecided neighbour outranks me in this round"
+    TravBuffers buf;
+    TravCtl *ctl;
+    int *sticky;
+};
+
+__device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v) {
+    return pu > pv || (pu == pv && u > v);
+}
+
+// Luby rounds with fixed priorities. Round r:
+//  edge pass over the undecided queue (merge-path expansion): for v undecided and each
+//      neighbour u != v: u in the set -> v out; u undecided and (prio,id)(u) > (prio,id)(v)
+//      -> v blocked in round r.
+//  vertex pass: undecided, not out, not blocked -> v joins; still undecided -> next queue.
+// A vertex joins exactly when every neighbour that outranks it is out, so the fixed point
+// is the greedy MIS in descending (priority, id) order: the set spmspvMis converges to
+// (src/spmspvMis.cuh:54-78: candidate if rand > threshold, select if rand > every
+// candidate neighbour's, knock out the neighbours), with ties broken by id instead of
+// left undecided.
+__global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
+    __shared__ Smem sm;
+    const int G = gridDim.x;
+    const int gtid = blockIdx.x * kBlock + threadIdx.x;
+    const int gstride = G * kBlock;
+    const int m = a.m;
+    for (int i = gtid; i < m; i += gstride) {
+        a.state[i] = kUndecided;
+        a.blocked[i] = 0;
+        a.buf.q0[i] = i;
+    }
+    if (gtid == 0) {
+        a.ctl->qlen[0] = m;
+        a.ctl->qlen[1] = 0;
+    }
+    if (!grid_barrier(a.ctl, a.sticky, kSiteMis)) return;
+
+    int cur = 0;
+    long long expanded = 0;
+    int round = 0;
+    for (;;) {
+        const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
+        if (nf == 0) break;
+        if (round > m + 1) {
+            if (gtid == 0) raise_error(a.ctl, a.sticky, APSPIE_ERR_NOT_CONVERGED, kSiteMisRoundCap);
+            break;
+        }
+        ++round;
+        int *qc = cur ? a.buf.q1 : a.buf.q0;
+        int *qn = cur ? a.buf.q0 : a.buf.q1;
+        int *qlen_next = &a.ctl->qlen[cur ^ 1];
+
+        frontier_phase_a<kBlock>(qc, nf, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum,
+                                 sm.scan_tmp, [&](int, int, int deg) { return deg; });
+        if (gtid == 0) *qlen_next = 0;
+        if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 1)) return;
+
+        const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
+        expanded += E;
+        const int *col = a.col_ind;
+        const unsigned *prio = a.prio;
+        unsigned char *state = a.state;
+        int *blocked = a.blocked;
+        const int r = round;
+        frontier_expand<kBlock, kVT>(
+            nf, E, a.buf.loc_off, a.buf.rs, sm,
+            [&](int j, int k, Smem &s) { s.aux[k] = __ldcg(qc + j); },
+            [&](bool valid, int k, int idx, Smem &s) {
+                if (!valid) return;
+                const int v = s.aux[k];
+                const int u = __ldg(col + idx);
+                if (u == v) return;
+                const unsigned char su = *reinterpret_cast<volatile unsigned char *>(state + u);
+                if (su == kIn) {
+                    state[v] = kOut;
+                } else if (su == kUndecided && outranks(__ldg(prio + u), u, __ldg(prio + v), v)) {
+                    blocked[v] = r;
+                }
+            });
+        if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 2)) return;
+
+        // vertex pass
+        for (int base = blockIdx.x * kBlock; base < nf; base += gstride) {
+            const int i = base + threadIdx.x;
+            bool keep = false;
+            int v = 0;
+            if (i < nf) {
+                v = __ldcg(qc + i);
+                const unsigned char s = __ldcg(state + v);
+                if (s == kUndecided) {
+                    if (__ldcg(blocked + v) != r)
+                        state[v] = kIn;
+                    else
+                        keep = true;
+                }
+            }
+            warp_append(keep, v, qn, qlen_next);
+        }
+        if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 3)) return;
+        cur ^= 1;
+    }
+    long long insz = 0;
+    for (int i = gtid; i < m; i += gstride) {
+        const unsigned char s = a.state[i];
+        a.member[i] = (s == kIn) ? 1 : 0;
+        insz += (s == kIn);
+    }
+    for (int o = 16; o; o >>= 1) insz += __shfl_down_sync(0xffffffffu, insz, o);
+    if ((threadIdx.x & 31) == 0 && insz)
+        atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->vertices_reached),
+                  static_cast<unsigned long long>(insz));
+    if (gtid == 0) {
+        a.ctl->iterations = round;
+        a.ctl->push_iterations = round;
+        a.ctl->edges_expanded = expanded;
+        a.ctl->edges_component = a.nnz;
+    }
+}
+
+// ================================================================================
+// one-hop boolean SpMSpV (MIS validity helper)
+// ================================================================================
+__global__ void spmspv_bool_kernel(int m, const int *__restrict__ row_ptr,
+                                   const int *__restrict__ col_ind, const int *__restrict__ x,
+                                   int *y) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int u = warp; u < m; u += nwarps) {
+        if (__ldg(x + u) == 0) continue;
+        const int r0 = __ldg(row_ptr + u), r1 = __ldg(row_ptr + u + 1);
+        for (int e = r0 + lane; e < r1; e += 32) y[__ldg(col_ind + e)] = 1;
+    }
+}
+
+apspie_status prepare_square(apspie_ctx *ctx, const apspie_csr *A, const char *who) {
+    apspie_status st = check_csr_view(ctx, A, who);
+    if (st != APSPIE_OK) return st;
+    if (A->m != A->n)
+        return set_error(ctx, APSPIE_ERR_INVALID_ARG, std::string(who) + ": matrix must be square");
+    if (A->m <= 0) return set_error(ctx, APSPIE_ERR_INVALID_ARG, std::string(who) + ": empty graph");
+    if (ctx->validate) {
+        st = validate_csr(ctx, A, true);
+        if (st != APSPIE_OK) return st;
+    }
+    return APSPIE_OK;
+}
+
+apspie_status reset_ctl(apspie_ctx *ctx) {
+    cudaError_t e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(TravCtl), ctx->stream);
+    return e == cudaSuccess ? APSPIE_OK : cuda_error(ctx, e, "control reset");
+}
+
+}  // namespace
+
+apspie_status trav_reserve(apspie_ctx *ctx, int m) {
+    void *base;
+    return scratch_reserve(ctx, trav_scratch_bytes(m) + static_cast<size_t>(m) * 5 + 512, &base);
+}
+
+}  // namespace apspie
+
+using namespace apspie;
+
+extern "C" {
+
+apspie_status apspie_ctx_reserve(apspie_ctx *ctx, int32_t m, int64_t nnz) {
+    (void)nnz;
+    if (!ctx || m < 0) return APSPIE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    return trav_reserve(ctx, m);
+}
+
+apspie_status apspie_bfs(apspie_ctx *ctx, const apspie_csr *A, int32_t source, int32_t depth_cap,
+                         int32_t *d_depth, apspie_run_stats *stats) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    apspie_status st = prepare_square(ctx, A, "apspie_bfs");
+    if (st != APSPIE_OK) return st;
+    if (source < 0 || source >= A->m)
+        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_bfs: source out of range");
+    if (!d_depth) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_bfs: NULL output");
+    void *base;
+    st = scratch_reserve(ctx, trav_scratch_bytes(A->m), &base);
+    if (st != APSPIE_OK) return st;
+    if ((st = reset_ctl(ctx)) != APSPIE_OK) return st;
+    BfsArgs a;
+    a.m = A->m;
+    a.nnz = A->nnz;
+    a.src = source;
+    a.depth_cap = depth_cap;
+    a.row_ptr = A->row_ptr;
+    a.col_ind = A->col_ind;
+    a.depth = d_depth;
+    a.buf = carve_trav(base, A->m);
+    a.ctl = ctx->d_ctl;
+    a.sticky = ctx->d_sticky_err;
+    a.alpha = ctx->bfs_alpha;
+    a.beta = ctx->bfs_beta;
+    void *args[] = {&a};
+    st = launch_persistent(ctx, reinterpret_cast<const void *>(bfs_kernel), kBlock, args, nullptr);
+    if (st != APSPIE_OK) return st;
+    return finish_call(ctx, stats, "apspie_bfs");
+}
+
+apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source, int32_t *d_dist,
+                          apspie_run_stats *stats) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    apspie_status st = prepare_square(ctx, A, "apspie_sssp");
+    if (st != APSPIE_OK) return st;
+    if (A->val_type != APSPIE_VAL_I32 || (A->nnz > 0 && !A->val))
+        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp: int32 edge weights required");
+    if (source < 0 || source >= A->m)
+        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp: source out of range");
+    if (!d_dist) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp: NULL output");
+    void *base;
+    st = scratch_reserve(ctx, trav_scratch_bytes(A->m), &base);
+    if (st != APSPIE_OK) return st;
+    if ((st = reset_ctl(ctx)) != APSPIE_OK) return st;
+    SsspArgs a;
+    a.m = A->m;
+    a.nnz = A->nnz;
+    a.src = source;
+    a.row_ptr = A->row_ptr;
+    a.col_ind = A->col_ind;
+    a.w = static_cast<const int *>(A->val);
+    a.dist = d_dist;
+    a.buf = carve_trav(base, A->m);
+    a.ctl = ctx->d_ctl;
+    a.sticky = ctx->d_sticky_err;
+    void *args[] = {&a};
+    st = launch_persistent(ctx, reinterpret_cast<const void *>(sssp_kernel), kBlock, args, nullptr);
+    if (st != APSPIE_OK) return st;
+    return finish_call(ctx, stats, "apspie_sssp");
+}
+
+apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
+                         uint8_t *d_member, apspie_run_stats *stats) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    apspie_status st = prepare_square(ctx, A, "apspie_mis");
+    if (st != APSPIE_OK) return st;
+    if (!d_priority || !d_member)
+        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_mis: NULL priority or output");
+    void *base;
+    const size_t tb = trav_scratch_bytes(A->m);
+    const size_t extra = Carver::need({static_cast<size_t>(A->m) * 4, static_cast<size_t>(A->m)});
+    st = scratch_reserve(ctx, tb + extra, &base);
+    if (st != APSPIE_OK) return st;
+    if ((st = reset_ctl(ctx)) != APSPIE_OK) return st;
+    MisArgs a;
+    a.m = A->m;
+    a.nnz = A->nnz;
+    a.row_ptr = A->row_ptr;
+    a.col_ind = A->col_ind;
+    a.prio = d_priority;
+    a.member = d_member;
+    a.buf = carve_trav(base, A->m);
+    Carver c(static_cast<char *>(base) + tb);
+    a.blocked = c.take<int>(A->m);
+    a.state = c.take<unsigned char>(A->m);
+    a.ctl = ctx->d_ctl;
+    a.sticky = ctx->d_sticky_err;
+    void *args[] = {&a};
+    st = launch_persistent(ctx, reinterpret_cast<const void *>(mis_kernel), kBlock, args, nullptr);
+    if (st != APSPIE_OK) return st;
+    return finish_call(ctx, stats, "apspie_mis");
+}
+
+apspie_status apspie_spmspv_bool(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_x,
+                                 int32_t *d_y) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    apspie_status st = check_csr_view(ctx, A, "apspie_spmspv_bool");
+    if (st != APSPIE_OK) return st;
+    if (!d_x || !d_y) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_spmspv_bool: NULL vector");
+    if (ctx->validate && (st = validate_csr(ctx, A, false)) != APSPIE_OK) return st;
+    cudaError_t e = cudaMemsetAsync(d_y, 0, static_cast<size_t>(A->n) * sizeof(int32_t), ctx->stream);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "spmspv_bool memset");
+    if (A->m > 0) {
+        spmspv_bool_kernel<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(A->m, A->row_ptr, A->col_ind,
+                                                                      d_x, d_y);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_error(ctx, e, "spmspv_bool launch");
+    }
+    return APSPIE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,259 @@
+"""Host graphs (numpy), device graphs (torch CUDA tensors) and the context wrapper.
+
+``Context`` wraps one ``apspie_ctx`` (device + stream + scratch arena). Its methods are
+thin forwards to the C ABI: every result comes from the library's CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _lib as L
+
+
+# ----------------------------------------------------------------------------------
+# host side
+# ----------------------------------------------------------------------------------
+@dataclass
+class HostGraph:
+    """CSR in host memory (int32 offsets/indices; values float32, int32 or None)."""
+
+    m: int
+    n: int
+    row_ptr: np.ndarray
+    col_ind: np.ndarray
+    val: Optional[np.ndarray] = None
+
+    @property
+    def nnz(self) -> int:
+        return int(self.col_ind.shape[0])
+
+    @property
+    def val_type(self) -> int:
+        if self.val is None:
+            return L.VAL_NONE
+        return L.VAL_F32 if self.val.dtype == np.float32 else L.VAL_I32
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.row_ptr)
+
+    def to_host_struct(self) -> L.HostCSR:
+        s = L.HostCSR()
+        s.m, s.n, s.nnz, s.val_type = self.m, self.n, self.nnz, self.val_type
+        self._keep = (np.ascontiguousarray(self.row_ptr, dtype=np.int32),
+                      np.ascontiguousarray(self.col_ind, dtype=np.int32))
+        s.row_ptr = self._keep[0].ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        s.col_ind = self._keep[1].ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        s.val = None
+        return s
+
+    def write_csr_file(self, path: str) -> None:
+        """Binary CSR file read by the oracle's reference driver."""
+        vt = self.val_type
+        with open(path, "wb") as f:
+            np.array([self.m, self.n, self.nnz, vt], dtype=np.int32).tofile(f)
+            self.row_ptr.astype(np.int32).tofile(f)
+            self.col_ind.astype(np.int32).tofile(f)
+            if self.val is not None:
+                self.val.tofile(f)
+
+
+def _from_struct(s: L.HostCSR) -> HostGraph:
+    m, nnz = s.m, s.nnz
+    rp = np.ctypeslib.as_array(s.row_ptr, shape=(m + 1,)).copy()
+    ci = np.ctypeslib.as_array(s.col_ind, shape=(max(nnz, 1),))[:nnz].copy()
+    val = None
+    if s.val_type == L.VAL_F32 and s.val:
+        val = np.ctypeslib.as_array(ctypes.cast(s.val, ctypes.POINTER(ctypes.c_float)),
+                                    shape=(max(nnz, 1),))[:nnz].copy()
+    elif s.val_type == L.VAL_I32 and s.val:
+        val = np.ctypeslib.as_array(ctypes.cast(s.val, ctypes.POINTER(ctypes.c_int32)),
+                                    shape=(max(nnz, 1),))[:nnz].copy()
+    L.lib().apspie_host_csr_free(ctypes.byref(s))
+    return HostGraph(m, s.n, rp, ci, val)
+
+
+def load_mtx(path: str, undirected: bool) -> HostGraph:
+    s = L.HostCSR()
+    L.check(L.lib().apspie_load_mtx(path.encode(), int(undirected), ctypes.byref(s)), None,
+            f"load_mtx({path})")
+    return _from_struct(s)
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, weight_seed: int = 3,
+             a: float = 0.57, b: float = 0.19, c: float = 0.19, weights: bool = True) -> HostGraph:
+    s = L.HostCSR()
+    L.check(L.lib().apspie_gen_rmat(scale, edge_factor, seed, weight_seed, a, b, c, int(weights),
+                                    ctypes.byref(s)), None, "gen_rmat")
+    return _from_struct(s)
+
+
+def gen_er(n: int, k: int = 8, seed: int = 5, val_type: int = L.VAL_F32) -> HostGraph:
+    s = L.HostCSR()
+    L.check(L.lib().apspie_gen_er(n, k, seed, val_type, ctypes.byref(s)), None, "gen_er")
+    return _from_struct(s)
+
+
+def mt19937_u32(seed: int, count: int) -> np.ndarray:
+    out = np.empty(count, dtype=np.uint32)
+    L.check(L.lib().apspie_mt19937_u32(seed, count, out.ctypes.data), None, "mt19937")
+    return out
+
+
+def max_degree_vertex(g: HostGraph) -> int:
+    return int(L.lib().apspie_max_degree_vertex(ctypes.byref(g.to_host_struct())))
+
+
+def lcc_sample(g: HostGraph, count: int, seed: int = 6) -> np.ndarray:
+    out = np.empty(count, dtype=np.int32)
+    L.check(L.lib().apspie_lcc_sample(ctypes.byref(g.to_host_struct()), count, seed,
+                                      out.ctypes.data), None, "lcc_sample")
+    return out
+
+
+def strict_lower(g: HostGraph) -> HostGraph:
+    s = L.HostCSR()
+    L.check(L.lib().apspie_csr_strict_lower(ctypes.byref(g.to_host_struct()), ctypes.byref(s)),
+            None, "strict_lower")
+    return _from_struct(s)
+
+
+# ----------------------------------------------------------------------------------
+# device side
+# ----------------------------------------------------------------------------------
+class DeviceGraph:
+    """CSR resident in HBM as torch CUDA tensors."""
+
+    def __init__(self, g: HostGraph, device="cuda"):
+        import torch
+
+        self.m, self.n, self.nnz = g.m, g.n, g.nnz
+        self.row_ptr = torch.from_numpy(np.ascontiguousarray(g.row_ptr, dtype=np.int32)).to(device)
+        self.col_ind = torch.from_numpy(np.ascontiguousarray(g.col_ind, dtype=np.int32)).to(device)
+        self.val = None if g.val is None else torch.from_numpy(np.ascontiguousarray(g.val)).to(device)
+        self.val_type = g.val_type
+
+    @classmethod
+    def from_tensors(cls, m: int, n: int, row_ptr, col_ind, val=None, val_type: int = L.VAL_NONE):
+        """Wraps existing device tensors (no copy)."""
+        self = cls.__new__(cls)
+        self.m, self.n, self.nnz = m, n, int(col_ind.shape[0])
+        self.row_ptr, self.col_ind, self.val = row_ptr, col_ind, val
+        self.val_type = val_type if val is not None else L.VAL_NONE
+        return self
+
+    def view(self, with_values: bool = True) -> L.CSR:
+        s = L.CSR()
+        s.m, s.n, s.nnz = self.m, self.n, self.nnz
+        s.row_ptr = self.row_ptr.data_ptr()
+        s.col_ind = self.col_ind.data_ptr() if self.nnz else None
+        if with_values and self.val is not None:
+            s.val_type = self.val_type
+            s.val = self.val.data_ptr()
+        else:
+            s.val_type = L.VAL_NONE
+            s.val = None
+        return s
+
+
+class Context:
+    """One apspie_ctx: a device, a CUDA stream (torch's current stream by default) and
+    the scratch arena reused by every call."""
+
+    def __init__(self, device: int = 0, stream=None):
+        import torch
+
+        torch.cuda.set_device(device)
+        self.device = device
+        self.stream = stream if stream is not None else torch.cuda.current_stream(device)
+        h = ctypes.c_void_p()
+        L.check(L.lib().apspie_ctx_create(device, ctypes.c_void_p(self.stream.cuda_stream),
+                                          ctypes.byref(h)), None, "ctx_create")
+        self.handle = h
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            L.lib().apspie_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- plumbing
+    def _check(self, st: int, what: str) -> None:
+        L.check(st, self.handle, what)
+
+    def synchronize(self) -> None:
+        self._check(L.lib().apspie_ctx_synchronize(self.handle), "synchronize")
+
+    def set_validate(self, on: bool) -> None:
+        self._check(L.lib().apspie_ctx_set_validate(self.handle, int(on)), "set_validate")
+
+    def set_bfs_tuning(self, alpha: float, beta: float) -> None:
+        self._check(L.lib().apspie_ctx_set_bfs_tuning(self.handle, alpha, beta), "set_bfs_tuning")
+
+    def reserve(self, m: int, nnz: int) -> None:
+        self._check(L.lib().apspie_ctx_reserve(self.handle, m, nnz), "reserve")
+
+    def scratch_bytes(self) -> int:
+        return int(L.lib().apspie_ctx_scratch_bytes(self.handle))
+
+    def validate(self, g: DeviceGraph) -> None:
+        self._check(L.lib().apspie_csr_validate(self.handle, ctypes.byref(g.view(False))), "validate")
+
+    # ---- algorithms (raw: caller-provided outputs, optional stats)
+    def bfs_into(self, g: DeviceGraph, source: int, out, depth_cap: int = 0, stats: bool = False):
+        st = L.RunStats() if stats else None
+        self._check(L.lib().apspie_bfs(self.handle, ctypes.byref(g.view(False)), source, depth_cap,
+                                       out.data_ptr(), ctypes.byref(st) if st else None), "bfs")
+        return st.as_dict() if st else None
+
+    def sssp_into(self, g: DeviceGraph, source: int, out, stats: bool = False):
+        st = L.RunStats() if stats else None
+        self._check(L.lib().apspie_sssp(self.handle, ctypes.byref(g.view(True)), source,
+                                        out.data_ptr(), ctypes.byref(st) if st else None), "sssp")
+        return st.as_dict() if st else None
+
+    def mis_into(self, g: DeviceGraph, prio, out, stats: bool = False):
+        st = L.RunStats() if stats else None
+        self._check(L.lib().apspie_mis(self.handle, ctypes.byref(g.view(False)), prio.data_ptr(),
+                                       out.data_ptr(), ctypes.byref(st) if st else None), "mis")
+        return st.as_dict() if st else None
+
+    def spmspv_bool_into(self, g: DeviceGraph, x, y) -> None:
+        self._check(L.lib().apspie_spmspv_bool(self.handle, ctypes.byref(g.view(False)),
+                                               x.data_ptr(), y.data_ptr()), "spmspv_bool")
+
+    # ---- convenience (allocate outputs)
+    def bfs(self, g: DeviceGraph, source: int, depth_cap: int = 0):
+        import torch
+
+        out = torch.empty(g.m, dtype=torch.int32, device=f"cuda:{self.device}")
+        self.bfs_into(g, source, out, depth_cap)
+        return out
+
+    def sssp(self, g: DeviceGraph, source: int):
+        import torch
+
+        out = torch.empty(g.m, dtype=torch.int32, device=f"cuda:{self.device}")
+        self.sssp_into(g, source, out)
+        return out
+
+    def mis(self, g: DeviceGraph, prio):
+        import torch
+
+        out = torch.empty(g.m, dtype=torch.uint8, device=f"cuda:{self.device}")
+        self.mis_into(g, prio, out)
+        return out

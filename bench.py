@@ -1,0 +1,438 @@
+"""Benchmark: single-source SSSP (min-plus SpMSpV) on R-MAT scale 20 -- the
+configuration the headline metric (BFS/SSSP GTEPS & % of HBM roofline) is quoted on --
+plus BFS on R-MAT scale 14 and MIS on R-MAT scale 20 as extra lines of the same JSON.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = one complete SSSP query from the max-degree vertex on the HBM-resident graph.
+`value` is device time (CUDA events on the library's stream, max over ranks); `e2e`
+goes through the C ABI with host buffers: every step uploads the CSR and weights from
+pinned host memory, runs the query and reads the distances back. Multi-GPU runs are
+independent replicas (a single-source query does not shard), so scaling is weak.
+`--impl reference` times the reference's own CPU SSSP (ssspCPU, compiled from the
+reference sources into oracle/_ref) on the same graph and source, one query per worker
+process per step on every host core it may use.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BFS/SSSP GTEPS & % HBM roofline; batched/served queries/s + p50/p99 vs plain"
+WORKLOAD = ("SSSP (min-plus SpMSpV) from the max-degree vertex on undirected R-MAT scale 20 "
+            "(1,048,576 vertices, edge factor 16, a/b/c/d .57/.19/.19/.05, seed 2, symmetrised, "
+            "deduplicated, int32 CSR), int32 weights uniform [1,255] from seed 3; int32 distances")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_graph(scale, seed):
+    import apspie_b200 as ap
+
+    g = ap.gen_rmat(scale, 16, seed, 3)
+    return g, ap.max_degree_vertex(g)
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_steps(stream, fn, steps):
+    """Runs fn() `steps` times between events on `stream`; returns (total_ms, per_step_ms list)."""
+    import torch
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for i in range(steps):
+        starts[i].record(stream)
+        fn()
+        ends[i].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1), [s.elapsed_time(e) for s, e in zip(starts, ends)]
+
+
+def traffic_from_profile(kernel: str):
+    """DRAM bytes per launch recorded by an ncu capture summarised under profiles/."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}.md")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------------
+def ref_worker_count():
+    n = os.cpu_count() or 1
+    try:
+        n = len(os.sched_getaffinity(0))
+    except Exception:
+        pass
+    return max(1, min(n, 32))
+
+
+def run_reference_sssp(g, src, workers, tmpdir):
+    """One step: `workers` concurrent reference ssspCPU processes on the same query.
+    Returns (max CPU ms over workers, distances of worker 0)."""
+    import oracle
+
+    gpath = os.path.join(tmpdir, "g.csr")
+    if not os.path.exists(gpath):
+        oracle._write_csr(gpath, g.row_ptr, g.col_ind, g.val)
+
+    def one(i):
+        out = os.path.join(tmpdir, f"d{i}.bin")
+        res = subprocess.run([oracle.REF_BIN, "sssp", gpath, str(src), out], capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(res.stderr[-300:])
+        for line in res.stdout.splitlines():
+            if line.startswith("APSPIE_REF "):
+                return json.loads(line[11:])["ms"]
+        raise RuntimeError("no timing line")
+
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        ms = list(ex.map(one, range(workers)))
+    return max(ms), np.fromfile(os.path.join(tmpdir, "d0.bin"), dtype=np.int32)
+
+
+def main_reference(args, ws, rank):
+    import oracle
+
+    if rank != 0:
+        return 0
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/apspie_ref (the reference CPU "
+                          "code compiled from its sources) was not built"}))
+        return 0
+    g, src = build_graph(20, 2)
+    comp_edges = int(g.degrees()[oracle.sssp(g.row_ptr, g.col_ind, g.val, src) >= 0].sum())
+    workers = ref_worker_count()
+    with tempfile.TemporaryDirectory() as d:
+        for _ in range(args.warmup):
+            run_reference_sssp(g, src, workers, d)
+        times = []
+        for _ in range(args.steps):
+            ms, _ = run_reference_sssp(g, src, workers, d)
+            times.append(ms)
+    ms_step = float(np.mean(times))
+    value = workers * comp_edges / (ms_step * 1e-3) / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": f"{workers} concurrent CPU queries"},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": workers, "kind": "reference",
+                         "sample": f"per step, {workers} concurrent runs of the reference ssspCPU "
+                                   "(src/testSssp.cpp:117, compiled from the reference sources) on the "
+                                   "full scale-20 query; CPU time inside each process"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------
+def main_ours(args, ws, rank, local):
+    import torch
+
+    import apspie_b200 as ap
+
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    g, src = build_graph(20, 2)
+    ctx = ap.Context(local)
+    stream = ctx.stream
+    dg = ap.DeviceGraph(g, dev)
+    out = torch.empty(g.m, dtype=torch.int32, device=dev)
+    ctx.reserve(g.m, g.nnz)
+
+    for _ in range(args.warmup):
+        ctx.sssp_into(dg, src, out)
+    st = ctx.sssp_into(dg, src, out, stats=True)
+    comp_edges, reached = st["edges_component"], st["vertices_reached"]
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(ws)
+    total_ms, per = time_steps(stream, lambda: ctx.sssp_into(dg, src, out), args.steps)
+    barrier(ws)
+    clocks = sampler.stop()
+    ctx.synchronize()
+    ms_step = max_over_ranks(ws, total_ms / args.steps)
+    launch_ms = max_over_ranks(ws, float(np.mean(per)))
+    value = ws * comp_edges / (ms_step * 1e-3) / 1e9
+
+    # e2e through the C ABI with host buffers
+    h_rp = torch.from_numpy(g.row_ptr).pin_memory()
+    h_ci = torch.from_numpy(g.col_ind).pin_memory()
+    h_w = torch.from_numpy(g.val).pin_memory()
+    h_out = torch.empty(g.m, dtype=torch.int32).pin_memory()
+    d_rp = torch.empty_like(h_rp, device=dev)
+    d_ci = torch.empty_like(h_ci, device=dev)
+    d_w = torch.empty_like(h_w, device=dev)
+    e2e_graph = ap.DeviceGraph.from_tensors(g.m, g.n, d_rp, d_ci, d_w, ap.VAL_I32)
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            d_rp.copy_(h_rp, non_blocking=True)
+            d_ci.copy_(h_ci, non_blocking=True)
+            d_w.copy_(h_w, non_blocking=True)
+        ctx.sssp_into(e2e_graph, src, out)
+        with torch.cuda.stream(stream):
+            h_out.copy_(out, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier(ws)
+    e2e_total, _ = time_steps(stream, e2e_step, args.steps)
+    barrier(ws)
+    e2e_ms = max_over_ranks(ws, e2e_total / args.steps)
+    h2d = (g.m + 1) * 4 + g.nnz * 8
+    d2h = g.m * 4
+
+    # correctness of what was timed
+    import oracle
+
+    ref = None
+    if rank == 0:
+        ref = oracle.sssp(g.row_ptr, g.col_ind, g.val, src)
+        assert np.array_equal(h_out.numpy(), ref), "timed SSSP result differs from the oracle"
+
+    peak, peak_kind = hbm_peak()
+    alg_bytes = 8 * comp_edges + 8 * reached + 4 * g.m
+    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (CSR + weights 256 MB > 126 MB)",
+                   "source": int(src), "vertices_reached": int(reached), "edges_component": int(comp_edges),
+                   "iterations": st["iterations"], "edges_relaxed": st["edges_expanded"]},
+        "e2e": {"value": ws * comp_edges / (e2e_ms * 1e-3) / 1e9, "unit": "GTEPS",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic_from_profile("sssp_kernel_rmat20"),
+                     "kernel": "sssp_kernel", "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                     if peak_kind == "measured" else "fallback 6650 GB/s",
+                     "alg_bytes_per_launch": alg_bytes, "launch_ms": launch_ms},
+        "clocks": clocks,
+    }
+
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(g, src, comp_edges)
+    if not args.no_extra:
+        line["extra"] = extras(ctx, args, ws, local)
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def cpu_baseline(g, src, comp_edges):
+    import oracle
+
+    if oracle.ref_available():
+        _, info = oracle.ref_sssp(g.row_ptr, g.col_ind, g.val, src)
+        ms, kind = info["ms"], "reference"
+        sample = "one full scale-20 SSSP query by the reference ssspCPU (src/testSssp.cpp:117) compiled from its sources"
+    else:
+        t0 = time.perf_counter()
+        oracle.sssp(g.row_ptr, g.col_ind, g.val, src)
+        ms, kind = (time.perf_counter() - t0) * 1e3, "port"
+        sample = "one full scale-20 SSSP query by the oracle's C restatement"
+    return {"value": comp_edges / (ms * 1e-3) / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind,
+            "sample": sample, "ms": ms}
+
+
+def extras(ctx, args, ws, local):
+    """BFS on R-MAT scale 14 (seed 1) and MIS on R-MAT scale 20 (seed 2), same timing rules."""
+    import torch
+
+    import apspie_b200 as ap
+    import oracle
+
+    dev = f"cuda:{local}"
+    res = {}
+    g14, s14 = build_graph(14, 1)
+    d14 = ap.DeviceGraph(g14, dev)
+    o14 = torch.empty(g14.m, dtype=torch.int32, device=dev)
+    for _ in range(max(3, args.warmup)):
+        ctx.bfs_into(d14, s14, o14)
+    st = ctx.bfs_into(d14, s14, o14, stats=True)
+    steps = max(args.steps, 50)
+    tot, per = time_steps(ctx.stream, lambda: ctx.bfs_into(d14, s14, o14), steps)
+    ms = max_over_ranks(ws, tot / steps)
+    res["bfs_rmat14"] = {"GTEPS": ws * st["edges_component"] / (ms * 1e-3) / 1e9, "us_per_bfs": ms * 1e3,
+                         "levels": st["iterations"], "push_levels": st["push_iterations"],
+                         "pull_levels": st["pull_iterations"], "edges_component": st["edges_component"],
+                         "source": int(s14), "steps": steps,
+                         "exact": bool(np.array_equal(o14.cpu().numpy(), oracle.bfs(g14.row_ptr, g14.col_ind, s14))),
+                         "note": "whole CSR (1.8 MB) is L2-resident: launch/latency bound"}
+    if oracle.ref_available():
+        _, info = oracle.ref_bfs(g14.row_ptr, g14.col_ind, s14)
+        res["bfs_rmat14"]["cpu_reference_ms"] = info["ms"]
+
+    g20, _ = build_graph(20, 2)
+    d20 = ap.DeviceGraph(g20, dev)
+    pr = ap.mt19937_u32(4, g20.m)
+    prio = torch.from_numpy(pr.view(np.int32)).to(dev)
+    mem = torch.empty(g20.m, dtype=torch.uint8, device=dev)
+    for _ in range(max(2, args.warmup)):
+        ctx.mis_into(d20, prio, mem)
+    st = ctx.mis_into(d20, prio, mem, stats=True)
+    steps = max(5, min(args.steps, 20))
+    tot, _ = time_steps(ctx.stream, lambda: ctx.mis_into(d20, prio, mem), steps)
+    ms = max_over_ranks(ws, tot / steps)
+    alg = 4 * g20.nnz + 13 * g20.m
+    res["mis_rmat20"] = {"ms": ms, "rounds": st["iterations"], "set_size": st["vertices_reached"],
+                         "edges_scanned": st["edges_expanded"], "alg_GBps": alg / (ms * 1e-3) / 1e9,
+                         "exact": bool(np.array_equal(mem.cpu().numpy(), oracle.mis_greedy(g20.row_ptr, g20.col_ind, pr)))}
+    # BFS at scale 20 for the roofline of the BFS kernel on an HBM-sized graph
+    s20 = ap.max_degree_vertex(g20)
+    o20 = torch.empty(g20.m, dtype=torch.int32, device=dev)
+    for _ in range(3):
+        ctx.bfs_into(d20, s20, o20)
+    st = ctx.bfs_into(d20, s20, o20, stats=True)
+    steps = max(args.steps, 20)
+    tot, _ = time_steps(ctx.stream, lambda: ctx.bfs_into(d20, s20, o20), steps)
+    ms = max_over_ranks(ws, tot / steps)
+    res["bfs_rmat20"] = {"GTEPS": ws * st["edges_component"] / (ms * 1e-3) / 1e9, "ms": ms,
+                         "levels": st["iterations"], "push_levels": st["push_iterations"],
+                         "pull_levels": st["pull_iterations"]}
+    return res
+
+
+def main():
+    ap_ = argparse.ArgumentParser()
+    ap_.add_argument("--gpus", type=int, default=1)
+    ap_.add_argument("--steps", type=int, default=20)
+    ap_.add_argument("--warmup", type=int, default=3)
+    ap_.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap_.add_argument("--no-extra", action="store_true")
+    ap_.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap_.parse_args()
+    ws, rank, local = dist_env()
+    if ws > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            return main_reference(args, ws, rank)
+        return main_ours(args, ws, rank, local)
+    finally:
+        if ws > 1 and args.impl == "ours":
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

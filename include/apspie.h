@@ -1,0 +1,139 @@
+/*
+ * apspie.h -- C ABI of the B200 (sm_100a) SpMSpV / hash-SpGEMM graph library.
+ *
+ * Every pointer named d_* is DEVICE memory on the context's GPU; h_* is host memory.
+ * All CSR structures are int32 (row offsets and column indices), as in the reference's
+ * d_matrix container (src/matrix.hpp:6-37: d_cscColPtr / d_cscRowInd / d_cscVal, which
+ * hold CSR despite their names).
+ *
+ * Conventions shared by every entry point:
+ *  - Calls never exit the process. They return an apspie_status; the message of the
+ *    last failure on a context is apspie_ctx_last_error(ctx).
+ *  - The caller owns input and output arrays. Scratch (frontier queues, bitmaps, hash
+ *    tables) is owned by the context, reused across calls and grown on demand; there is
+ *    no per-level or per-iteration allocation.
+ *  - Calls are enqueued on the context's stream. Those that return a host scalar
+ *    (triangle count, nnz(C), run statistics) synchronise that stream.
+ *  - A context is not thread-safe; distinct contexts are independent.
+ *  - Termination is decided on the device (empty frontier / no change). The reference's
+ *    `depth` argument is kept as a level cap: depth <= 0 means unlimited.
+ */
+#ifndef APSPIE_H
+#define APSPIE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum apspie_status {
+    APSPIE_OK = 0,
+    APSPIE_ERR_INVALID_ARG = 1,   /* bad pointer, size, source, or CSR contents */
+    APSPIE_ERR_OOM = 2,           /* device allocation failed */
+    APSPIE_ERR_HASH_OVERFLOW = 3, /* a hash table ran out of probes (spgemmKernel.cuh:335) */
+    APSPIE_ERR_TIMEOUT = 4,       /* a bounded device-side wait ran out */
+    APSPIE_ERR_CUDA = 5,          /* a CUDA runtime call failed */
+    APSPIE_ERR_UNSUPPORTED = 6,   /* valid request this build does not serve */
+    APSPIE_ERR_NOT_CONVERGED = 7  /* iteration cap reached before the fixed point */
+} apspie_status;
+
+typedef enum apspie_val_type {
+    APSPIE_VAL_NONE = 0, /* pattern only (boolean semiring) */
+    APSPIE_VAL_F32 = 1,
+    APSPIE_VAL_I32 = 2
+} apspie_val_type;
+
+/* Device-resident CSR matrix view (not owned). */
+typedef struct apspie_csr {
+    int32_t m;             /* rows */
+    int32_t n;             /* columns */
+    int32_t nnz;           /* stored entries */
+    int32_t val_type;      /* apspie_val_type of `val` */
+    const int32_t *row_ptr; /* d, m+1 */
+    const int32_t *col_ind; /* d, nnz */
+    const void *val;        /* d, nnz elements of val_type, or NULL */
+} apspie_csr;
+
+/* Device-resident CSR matrix allocated by the library (spgemm output); release with
+ * apspie_csr_free. Mirrors the callee-allocated C of spgemm.cuh:202-204 / tc.cuh:73,120. */
+typedef struct apspie_csr_owned {
+    int32_t m, n, nnz, val_type;
+    int32_t *row_ptr;
+    int32_t *col_ind;
+    void *val;
+} apspie_csr_owned;
+
+/* Per-call statistics (filled only when a non-NULL pointer is passed; that call then
+ * synchronises the stream). */
+typedef struct apspie_run_stats {
+    int32_t iterations;        /* BFS levels / SSSP iterations / MIS rounds executed */
+    int32_t push_iterations;   /* iterations expanded top-down (push) */
+    int32_t pull_iterations;   /* iterations expanded bottom-up (pull) */
+    int32_t reserved;
+    int64_t edges_expanded;    /* sum of deg(v) over every frontier expansion (re-expansions counted) */
+    int64_t edges_component;   /* sum of deg(v) over reached vertices: the GTEPS numerator */
+    int64_t vertices_reached;
+} apspie_run_stats;
+
+typedef struct apspie_ctx apspie_ctx;
+
+/* ---- context ------------------------------------------------------------------ */
+
+/* Creates a context on `device`, enqueuing on `cuda_stream` (a cudaStream_t; NULL = the
+ * legacy default stream). Replaces the reference's mgpu::CudaContext (test/bfs/main.cu:27). */
+apspie_status apspie_ctx_create(int device, void *cuda_stream, apspie_ctx **out);
+void apspie_ctx_destroy(apspie_ctx *ctx);
+const char *apspie_ctx_last_error(const apspie_ctx *ctx);
+apspie_status apspie_ctx_synchronize(apspie_ctx *ctx);
+/* Pre-sizes the scratch arena for graphs up to m vertices and nnz entries. */
+apspie_status apspie_ctx_reserve(apspie_ctx *ctx, int32_t m, int64_t nnz);
+/* When on (default off), every traversal entry point first checks its CSR on the device
+ * (offsets monotone, first 0, last nnz, columns in range) and returns
+ * APSPIE_ERR_INVALID_ARG instead of touching a malformed graph. */
+apspie_status apspie_ctx_set_validate(apspie_ctx *ctx, int on);
+/* Direction-switch thresholds for BFS (Beamer's alpha/beta; defaults 14 and 24).
+ * alpha <= 0 forces push on every level. */
+apspie_status apspie_ctx_set_bfs_tuning(apspie_ctx *ctx, float alpha, float beta);
+/* Bytes of device scratch the context currently holds. */
+int64_t apspie_ctx_scratch_bytes(const apspie_ctx *ctx);
+
+/* Checks a CSR on the device; APSPIE_OK or APSPIE_ERR_INVALID_ARG. */
+apspie_status apspie_csr_validate(apspie_ctx *ctx, const apspie_csr *A);
+
+/* ---- traversal (SpMSpV) --------------------------------------------------------- */
+
+/* Level-synchronous BFS by boolean OR-AND SpMSpV with a push/pull switch.
+ * d_depth[m] (int32, caller-allocated): hop count from `source`, -1 unreached.
+ * Replaces spmspvBfs (src/spmspvBfs.cuh:96) and bfs<T> (src/bfs.cuh:33). */
+apspie_status apspie_bfs(apspie_ctx *ctx, const apspie_csr *A, int32_t source,
+                         int32_t depth_cap, int32_t *d_depth, apspie_run_stats *stats);
+
+/* Single-source shortest paths by min-plus SpMSpV over int32 edge weights >= 0
+ * (A->val_type == APSPIE_VAL_I32), iterated on the device to the fixed point.
+ * d_dist[m] (int32): distance, -1 unreached (the CPU check's convention,
+ * src/testSssp.cpp:50). Replaces sssp<Value> (src/sssp.cuh:28) and
+ * spmspvSssp (src/spmspvSssp.cuh:92). Returns APSPIE_ERR_INVALID_ARG when a path
+ * length would exceed INT32_MAX - 1. */
+apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source,
+                          int32_t *d_dist, apspie_run_stats *stats);
+
+/* Maximal independent set with fixed priorities: the set a priority-thresholded Luby
+ * loop converges to (src/spmspvMis.cuh:149-344), i.e. the greedy MIS in descending
+ * (priority, vertex id) order. d_member[m] (uint8): 1 in the set, 0 not. A must be
+ * symmetric; self-loops are ignored. */
+apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
+                         uint8_t *d_member, apspie_run_stats *stats);
+
+/* One-hop boolean SpMSpV y = A^T x over a dense 0/1 int32 vector: d_y[v] = 1 if some
+ * u with d_x[u] != 0 has v in its row, else 0. Replaces spmspvCsr
+ * (src/spmspvMis.cuh:81), the reference's MIS validity helper. */
+apspie_status apspie_spmspv_bool(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_x,
+                                 int32_t *d_y);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APSPIE_H */
