@@ -37,10 +37,14 @@ class ApspieError(RuntimeError):
         self.name = STATUS.get(status, str(status))
 
 
+CSR_SYMMETRIC = 1
+
+
 class CSR(ctypes.Structure):
     _fields_ = [
         ("m", c_int32), ("n", c_int32), ("nnz", c_int32), ("val_type", c_int32),
         ("row_ptr", c_void_p), ("col_ind", c_void_p), ("val", c_void_p),
+        ("flags", c_uint32), ("reserved", c_uint32),
     ]
 
 
@@ -79,6 +83,8 @@ SIGNATURES = {
     "apspie_ctx_reserve": (c_int, [c_void_p, c_int32, c_int64]),
     "apspie_ctx_set_validate": (c_int, [c_void_p, c_int]),
     "apspie_ctx_set_bfs_tuning": (c_int, [c_void_p, c_float, c_float]),
+    "apspie_ctx_set_sssp_delta": (c_int, [c_void_p, c_int32]),
+    "apspie_ctx_set_max_grid": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_scratch_bytes": (c_int64, [c_void_p]),
     "apspie_csr_validate": (c_int, [c_void_p, POINTER(CSR)]),
     # traversal

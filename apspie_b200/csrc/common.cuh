@@ -24,7 +24,8 @@ struct TravCtl {
     int iterations;
     int push_iterations;
     int pull_iterations;
-    int pad0;
+    int flen[2];         // far-pile lengths (SSSP, ping-pong)
+    int delta;           // SSSP bucket width in use
     long long edges_expanded;
     long long edges_component;
     long long vertices_reached;
@@ -54,6 +55,8 @@ struct apspie_ctx {
     int validate = 0;
     float bfs_alpha = 14.0f;
     float bfs_beta = 24.0f;
+    int sssp_delta = 0;  // <= 0: chosen on the device
+    int max_grid = 0;    // 0: as many co-resident blocks as fit
 };
 
 namespace apspie {

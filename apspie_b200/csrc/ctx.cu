@@ -122,6 +122,7 @@ apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, vo
     if (per_sm < 1) return set_error(ctx, APSPIE_ERR_CUDA, "persistent kernel cannot be resident");
     int grid = per_sm * ctx->num_sms;
     if (grid > max_grid) grid = max_grid;
+    if (ctx->max_grid > 0 && grid > ctx->max_grid) grid = ctx->max_grid;
     if (grid > kMaxGrid) grid = kMaxGrid;
     e = cudaLaunchCooperativeKernel(func, dim3(grid), dim3(block), args, 0, ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "cooperative launch");
@@ -236,6 +237,18 @@ apspie_status apspie_ctx_set_bfs_tuning(apspie_ctx *ctx, float alpha, float beta
     if (!(beta > 0.0f)) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "beta must be > 0");
     ctx->bfs_alpha = alpha;
     ctx->bfs_beta = beta;
+    return APSPIE_OK;
+}
+
+apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    ctx->sssp_delta = delta;
+    return APSPIE_OK;
+}
+
+apspie_status apspie_ctx_set_max_grid(apspie_ctx *ctx, int32_t max_blocks) {
+    if (!ctx || max_blocks < 0) return APSPIE_ERR_INVALID_ARG;
+    ctx->max_grid = max_blocks;
     return APSPIE_OK;
 }
 

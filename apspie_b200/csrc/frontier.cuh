@@ -23,6 +23,8 @@
 
 namespace apspie {
 
+constexpr int kSplitBatch = 256;
+
 template <int BLOCK, int VT>
 struct ExpandSmem {
     static constexpr int NV = BLOCK * VT;
@@ -32,7 +34,7 @@ struct ExpandSmem {
     int aux[NV + 1];         // per-entry payload (vertex id, distance, ...)
     int seg[NV];             // tile edge slot -> staged entry
     int scan_tmp[33];
-    long long split[2];
+    int tsplit[kSplitBatch + 1];  // merge-path split of each tile of the current batch
 };
 
 // Phase A over this block's chunk of queue q[0, nf). hook(i, v, deg) may rewrite the
@@ -110,6 +112,10 @@ __device__ __forceinline__ int frontier_merge_path(long long diag, int nf, int E
 // handles the edge at CSR position idx owned by staged entry k. `op` is called by every
 // thread of the block the same number of times (valid=false for idle slots), so it may
 // use warp collectives.
+//
+// Block b owns a contiguous run of tiles. The split points of up to kSplitBatch tiles are
+// found in parallel (one binary search per thread) before the tiles are walked, so the
+// dependent global-memory search latency is paid once per batch rather than per tile.
 template <int BLOCK, int VT, class Load, class Op>
 __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__restrict__ loc_off,
                                                 const int *__restrict__ rs,
@@ -119,64 +125,73 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
     const int C = (nf + G - 1) / G;
     const long long total = static_cast<long long>(nf) + E;
     const long long ntiles = (total + NV - 1) / NV;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += G) {
-        const long long d0 = tile * NV;
-        const long long d1 = d0 + NV < total ? d0 + NV : total;
-        if (threadIdx.x == 0) sm.split[0] = frontier_merge_path(d0, nf, E, loc_off, sm.base, C);
-        if (threadIdx.x == 32) sm.split[1] = frontier_merge_path(d1, nf, E, loc_off, sm.base, C);
-        __syncthreads();
-        const int a0 = static_cast<int>(sm.split[0]);
-        const int a1 = static_cast<int>(sm.split[1]);
-        const int e0 = static_cast<int>(d0 - a0);
-        const int e1 = static_cast<int>(d1 - a1);
-        const int jb = a0 > 0 ? a0 - 1 : 0;
-        const int ne = a1 - jb;
-        for (int k = threadIdx.x; k < ne; k += BLOCK) {
-            const int j = jb + k;
-            sm.off[k] = sm.base[j / C] + __ldcg(loc_off + j);
-            sm.rs[k] = __ldcg(rs + j);
-            load(j, k, sm);
+    const long long per = (ntiles + G - 1) / G;
+    const long long t_begin = static_cast<long long>(blockIdx.x) * per;
+    const long long t_end = t_begin + per < ntiles ? t_begin + per : ntiles;
+    for (long long tb = t_begin; tb < t_end; tb += kSplitBatch) {
+        const long long te = tb + kSplitBatch < t_end ? tb + kSplitBatch : t_end;
+        for (int s = threadIdx.x; s <= te - tb; s += BLOCK) {
+            long long d = (tb + s) * NV;
+            if (d > total) d = total;
+            sm.tsplit[s] = frontier_merge_path(d, nf, E, loc_off, sm.base, C);
         }
         __syncthreads();
-        const int tcount = static_cast<int>(d1 - d0);
-        const int diag = threadIdx.x * VT;
-        if (diag < tcount) {
-            const int acount = a1 - a0, bcount = e1 - e0;
-            int lo = diag - bcount > 0 ? diag - bcount : 0;
-            int hi = diag < acount ? diag : acount;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (sm.off[a0 + mid - jb] <= e0 + diag - 1 - mid)
-                    lo = mid + 1;
-                else
-                    hi = mid;
+        for (long long tile = tb; tile < te; ++tile) {
+            const long long d0 = tile * NV;
+            const long long d1 = d0 + NV < total ? d0 + NV : total;
+            const int a0 = sm.tsplit[tile - tb];
+            const int a1 = sm.tsplit[tile - tb + 1];
+            const int e0 = static_cast<int>(d0 - a0);
+            const int e1 = static_cast<int>(d1 - a1);
+            const int jb = a0 > 0 ? a0 - 1 : 0;
+            const int ne = a1 - jb;
+            for (int k = threadIdx.x; k < ne; k += BLOCK) {
+                const int j = jb + k;
+                sm.off[k] = sm.base[j / C] + __ldcg(loc_off + j);
+                sm.rs[k] = __ldcg(rs + j);
+                load(j, k, sm);
             }
-            int ja = a0 + lo, eb = e0 + diag - lo;
-            int cur = ja - 1 - jb;
-            const int end = diag + VT < tcount ? diag + VT : tcount;
-            for (int it = diag; it < end; ++it) {
-                if (ja < a1 && sm.off[ja - jb] <= eb) {
-                    cur = ja - jb;
-                    ++ja;
-                } else {
-                    sm.seg[eb - e0] = cur;
-                    ++eb;
+            __syncthreads();
+            const int tcount = static_cast<int>(d1 - d0);
+            const int diag = threadIdx.x * VT;
+            if (diag < tcount) {
+                const int acount = a1 - a0, bcount = e1 - e0;
+                int lo = diag - bcount > 0 ? diag - bcount : 0;
+                int hi = diag < acount ? diag : acount;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (sm.off[a0 + mid - jb] <= e0 + diag - 1 - mid)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                int ja = a0 + lo, eb = e0 + diag - lo;
+                int cur = ja - 1 - jb;
+                const int end = diag + VT < tcount ? diag + VT : tcount;
+                for (int it = diag; it < end; ++it) {
+                    if (ja < a1 && sm.off[ja - jb] <= eb) {
+                        cur = ja - jb;
+                        ++ja;
+                    } else {
+                        sm.seg[eb - e0] = cur;
+                        ++eb;
+                    }
                 }
             }
-        }
-        __syncthreads();
-        const int ned = e1 - e0;
-        for (int k0 = 0; k0 < ned; k0 += BLOCK) {
-            const int el = k0 + threadIdx.x;
-            const bool valid = el < ned;
-            int k = 0, idx = 0;
-            if (valid) {
-                k = sm.seg[el];
-                idx = sm.rs[k] + (e0 + el - sm.off[k]);
+            __syncthreads();
+            const int ned = e1 - e0;
+            for (int k0 = 0; k0 < ned; k0 += BLOCK) {
+                const int el = k0 + threadIdx.x;
+                const bool valid = el < ned;
+                int k = 0, idx = 0;
+                if (valid) {
+                    k = sm.seg[el];
+                    idx = sm.rs[k] + (e0 + el - sm.off[k]);
+                }
+                op(valid, k, idx, sm);
             }
-            op(valid, k, idx, sm);
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 

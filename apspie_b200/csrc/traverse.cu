@@ -33,15 +33,15 @@ enum : int {
 };
 
 struct TravBuffers {
-    int *q0, *q1, *rs, *loc_off, *chunk_sum, *aux;
+    int *q0, *q1, *q2, *q3, *rs, *loc_off, *chunk_sum, *aux, *aux2;
     unsigned *bits0, *bits1, *bits2;
 };
 
 size_t trav_scratch_bytes(int m) {
     const size_t words = (static_cast<size_t>(m) + 31) / 32;
     const size_t mi = static_cast<size_t>(m) + 1;
-    return Carver::need({mi * 4, mi * 4, mi * 4, mi * 4, kMaxGrid * 4, mi * 4, words * 4,
-                         words * 4, words * 4});
+    return Carver::need({mi * 4, mi * 4, mi * 4, mi * 4, mi * 4, mi * 4, kMaxGrid * 4, mi * 4,
+                         mi * 4, words * 4, words * 4, words * 4});
 }
 
 TravBuffers carve_trav(void *base, int m) {
@@ -51,10 +51,13 @@ TravBuffers carve_trav(void *base, int m) {
     TravBuffers b;
     b.q0 = c.take<int>(mi);
     b.q1 = c.take<int>(mi);
+    b.q2 = c.take<int>(mi);
+    b.q3 = c.take<int>(mi);
     b.rs = c.take<int>(mi);
     b.loc_off = c.take<int>(mi);
     b.chunk_sum = c.take<int>(kMaxGrid);
     b.aux = c.take<int>(mi);
+    b.aux2 = c.take<int>(mi);
     b.bits0 = c.take<unsigned>(words);
     b.bits1 = c.take<unsigned>(words);
     b.bits2 = c.take<unsigned>(words);
@@ -73,6 +76,7 @@ struct BfsArgs {
     TravCtl *ctl;
     int *sticky;
     float alpha, beta;
+    int allow_pull;  // pattern declared symmetric
 };
 
 // Level-synchronous BFS. Level L discovers the vertices at hop distance L.
@@ -136,7 +140,8 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
         expanded += E;
         const long long m_u = static_cast<long long>(a.nnz) - visited_edges;
         if (!pull) {
-            if (a.alpha > 0.0f && static_cast<double>(E) > static_cast<double>(m_u) / a.alpha)
+            if (a.allow_pull && a.alpha > 0.0f &&
+                static_cast<double>(E) > static_cast<double>(m_u) / a.alpha)
                 pull = true;
         } else if (static_cast<double>(nf) < static_cast<double>(m) / a.beta) {
             pull = false;
@@ -212,23 +217,29 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
 // SSSP
 // ================================================================================
 struct SsspArgs {
-    int m, nnz, src;
+    int m, nnz, src, delta_hint;
     const int *__restrict__ row_ptr;
     const int *__restrict__ col_ind;
     const int *__restrict__ w;
     int *dist;
-    TravBuffers buf;  // bits0 = "queued for next iteration"; aux = distance snapshot
+    // bits0 = queued in the near frontier, bits1 = held in the far pile;
+    // q0/q1 near queues, q2/q3 far piles, aux = distance snapshot of each near entry,
+    // aux2 = distance each vertex was last expanded with
+    TravBuffers buf;
     TravCtl *ctl;
     int *sticky;
 };
 
-// Frontier Bellman-Ford with min-plus SpMSpV: the frontier is the set of vertices whose
-// distance dropped in the previous iteration (the reference's dense "every finite entry"
-// frontier, src/spmspvSssp.cuh:31-36, restricted to the changed ones). A relaxation is a
-// plain read of dist[v] and, only if it improves, an atomicMin; the winner of the
-// queued-bit test-and-set appends v to the next queue. The result is the fixed point
-// (exact shortest distances for non-negative integer weights), independent of the order
-// in which relaxations land.
+// Min-plus SpMSpV iterated to the fixed point with near/far buckets (delta-stepping in
+// the near-far form): the frontier holds the vertices whose distance dropped below the
+// current threshold T; a relaxation that lands at or above T parks the vertex on the far
+// pile instead. When the near frontier empties, T advances by delta and the far pile is
+// split into the new near frontier and what stays far. A vertex is expanded again only
+// if its distance changed since its last expansion. The reference expands every finite
+// vertex each iteration (src/spmspvSssp.cuh:31-36, sort + ReduceByKey(min) :220-232) and
+// stops after the CPU BFS depth; here a relaxation is a plain read of dist[v] and, only
+// if it improves, an atomicMin, and the loop ends when both piles are empty. The result is
+// the exact fixed point for non-negative integer weights, independent of relaxation order.
 __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     __shared__ Smem sm;
     const int G = gridDim.x;
@@ -237,37 +248,100 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     const int m = a.m;
     const int words = (m + 31) >> 5;
     unsigned *inq = a.buf.bits0;
+    unsigned *infar = a.buf.bits1;
+    int *last = a.buf.aux2;
 
-    for (int i = gtid; i < m; i += gstride) a.dist[i] = (i == a.src) ? 0 : kInf;
-    for (int w = gtid; w < words; w += gstride) inq[w] = (w == (a.src >> 5)) ? (1u << (a.src & 31)) : 0u;
+    for (int i = gtid; i < m; i += gstride) {
+        a.dist[i] = (i == a.src) ? 0 : kInf;
+        last[i] = -1;
+    }
+    for (int w = gtid; w < words; w += gstride) {
+        inq[w] = (w == (a.src >> 5)) ? (1u << (a.src & 31)) : 0u;
+        infar[w] = 0u;
+    }
+    // sample the weights for the default bucket width
+    constexpr int kSample = 1 << 16;
+    const int nsamp = a.nnz < kSample ? a.nnz : kSample;
+    if (a.delta_hint <= 0) {
+        long long ws = 0;
+        for (int k = gtid; k < nsamp; k += gstride)
+            ws += __ldg(a.w + static_cast<long long>(k) * a.nnz / nsamp);
+        for (int o = 16; o; o >>= 1) ws += __shfl_down_sync(0xffffffffu, ws, o);
+        if ((threadIdx.x & 31) == 0 && ws)
+            atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->aux[0]),
+                      static_cast<unsigned long long>(ws));
+    }
     if (gtid == 0) {
         a.buf.q0[0] = a.src;
         a.ctl->qlen[0] = 1;
         a.ctl->qlen[1] = 0;
+        a.ctl->flen[0] = 0;
+        a.ctl->flen[1] = 0;
     }
     if (!grid_barrier(a.ctl, a.sticky, kSiteSssp)) return;
 
-    int cur = 0;
+    long long delta = a.delta_hint;
+    if (delta <= 0) {
+        const double mean_w = nsamp ? static_cast<double>(__ldcg(&a.ctl->aux[0])) / nsamp : 1.0;
+        const double mean_deg = m ? static_cast<double>(a.nnz) / m : 1.0;
+        delta = static_cast<long long>(32.0 * mean_w / (mean_deg > 1.0 ? mean_deg : 1.0));
+        if (delta < 1) delta = 1;
+    }
+    long long thresh = delta;
+    int cur = 0, fc = 0;
     long long expanded = 0;
-    int iters = 0;
+    int iters = 0, steps = 0;
+    const long long step_cap = 4LL * m + 4096;
     for (;;) {
-        const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
-        if (nf == 0) break;
-        if (iters > m + 1) {  // cannot happen with non-negative weights
+        if (++steps > step_cap) {
             if (gtid == 0) raise_error(a.ctl, a.sticky, APSPIE_ERR_NOT_CONVERGED, kSiteSsspIterCap);
             break;
         }
+        const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
         int *qc = cur ? a.buf.q1 : a.buf.q0;
         int *qn = cur ? a.buf.q0 : a.buf.q1;
+        int *fcur = fc ? a.buf.q3 : a.buf.q2;
+        int *fnext = fc ? a.buf.q2 : a.buf.q3;
+        int *dist = a.dist;
+        if (nf == 0) {
+            // near frontier empty: advance the threshold and split the far pile
+            const int nfar = ld_volatile_i32(&a.ctl->flen[fc]);
+            if (nfar == 0) break;
+            thresh += delta;
+            for (int base = blockIdx.x * kBlock; base < nfar; base += gstride) {
+                const int i = base + threadIdx.x;
+                bool to_near = false, stay = false;
+                int v = 0;
+                if (i < nfar) {
+                    v = __ldcg(fcur + i);
+                    const int d = __ldcg(dist + v);
+                    if (d < thresh) {
+                        atomicAnd(infar + (v >> 5), ~(1u << (v & 31)));
+                        const unsigned bit = 1u << (v & 31);
+                        to_near = !(atomicOr(inq + (v >> 5), bit) & bit);
+                    } else {
+                        stay = true;
+                    }
+                }
+                warp_append(to_near, v, qc, &a.ctl->qlen[cur]);
+                warp_append(stay, v, fnext, &a.ctl->flen[fc ^ 1]);
+            }
+            if (!grid_barrier(a.ctl, a.sticky, kSiteSssp + 3)) return;
+            if (gtid == 0) a.ctl->flen[fc] = 0;  // drained; every block read nfar above
+            fc ^= 1;
+            continue;
+        }
         int *qlen_next = &a.ctl->qlen[cur ^ 1];
         int *snap = a.buf.aux;
-        int *dist = a.dist;
 
-        // phase A: dequeue (clear queued bit), snapshot distance, degrees
+        // phase A: dequeue (clear queued bit), snapshot distance, skip unchanged vertices
         frontier_phase_a<kBlock>(qc, nf, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum,
                                  sm.scan_tmp, [&](int i, int v, int deg) {
                                      atomicAnd(inq + (v >> 5), ~(1u << (v & 31)));
-                                     snap[i] = __ldcg(dist + v);
+                                     const int d = __ldcg(dist + v);
+                                     snap[i] = d;
+                                     if (__ldcg(last + v) == d) return 0;
+                                     last[v] = d;
                                      return deg;
                                  });
         if (gtid == 0) *qlen_next = 0;
@@ -280,11 +354,13 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
         const int *wt = a.w;
         TravCtl *ctl = a.ctl;
         int *sticky = a.sticky;
+        int *flen = &a.ctl->flen[fc];
+        const long long T = thresh;
         frontier_expand<kBlock, kVT>(
             nf, E, a.buf.loc_off, a.buf.rs, sm,
             [&](int j, int k, Smem &s) { s.aux[k] = __ldcg(snap + j); },
             [&](bool valid, int k, int idx, Smem &s) {
-                bool fresh = false;
+                bool near = false, far = false;
                 int v = 0;
                 if (valid) {
                     v = __ldg(col + idx);
@@ -296,17 +372,21 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                         raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSsspOverflow);
                     } else {
                         const int ndi = static_cast<int>(nd);
-                        if (ndi < __ldcg(dist + v)) {
+                        // a stale (larger) cached value only costs an extra atomic
+                        if (ndi < dist[v]) {
                             const int old = atomicMin(dist + v, ndi);
                             if (ndi < old) {
                                 const unsigned bit = 1u << (v & 31);
-                                const unsigned ob = atomicOr(inq + (v >> 5), bit);
-                                fresh = !(ob & bit);
+                                if (nd < T)
+                                    near = !(atomicOr(inq + (v >> 5), bit) & bit);
+                                else
+                                    far = !(atomicOr(infar + (v >> 5), bit) & bit);
                             }
                         }
                     }
                 }
-                warp_append(fresh, v, qn, qlen_next);
+                warp_append(near, v, qn, qlen_next);
+                warp_append(far, v, fcur, flen);
             });
         if (!grid_barrier(a.ctl, a.sticky, kSiteSssp + 2)) return;
         cur ^= 1;
@@ -335,7 +415,9 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     if (gtid == 0) {
         a.ctl->iterations = iters;
         a.ctl->push_iterations = iters;
+        a.ctl->pull_iterations = steps - 1 - iters;  // threshold advances
         a.ctl->edges_expanded = expanded;
+        a.ctl->delta = static_cast<int>(delta);
     }
 }
 
@@ -550,6 +632,7 @@ apspie_status apspie_bfs(apspie_ctx *ctx, const apspie_csr *A, int32_t source, i
     a.sticky = ctx->d_sticky_err;
     a.alpha = ctx->bfs_alpha;
     a.beta = ctx->bfs_beta;
+    a.allow_pull = (A->flags & APSPIE_CSR_SYMMETRIC) ? 1 : 0;
     void *args[] = {&a};
     st = launch_persistent(ctx, reinterpret_cast<const void *>(bfs_kernel), kBlock, args, nullptr);
     if (st != APSPIE_OK) return st;
@@ -579,6 +662,7 @@ apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source, 
     a.col_ind = A->col_ind;
     a.w = static_cast<const int *>(A->val);
     a.dist = d_dist;
+    a.delta_hint = ctx->sssp_delta;
     a.buf = carve_trav(base, A->m);
     a.ctl = ctx->d_ctl;
     a.sticky = ctx->d_sticky_err;

@@ -26,6 +26,7 @@ class HostGraph:
     row_ptr: np.ndarray
     col_ind: np.ndarray
     val: Optional[np.ndarray] = None
+    symmetric: bool = False  # pattern known to be symmetric (undirected graph)
 
     @property
     def nnz(self) -> int:
@@ -61,7 +62,7 @@ class HostGraph:
                 self.val.tofile(f)
 
 
-def _from_struct(s: L.HostCSR) -> HostGraph:
+def _from_struct(s: L.HostCSR, symmetric: bool = False) -> HostGraph:
     m, nnz = s.m, s.nnz
     rp = np.ctypeslib.as_array(s.row_ptr, shape=(m + 1,)).copy()
     ci = np.ctypeslib.as_array(s.col_ind, shape=(max(nnz, 1),))[:nnz].copy()
@@ -72,15 +73,16 @@ def _from_struct(s: L.HostCSR) -> HostGraph:
     elif s.val_type == L.VAL_I32 and s.val:
         val = np.ctypeslib.as_array(ctypes.cast(s.val, ctypes.POINTER(ctypes.c_int32)),
                                     shape=(max(nnz, 1),))[:nnz].copy()
+    n = s.n
     L.lib().apspie_host_csr_free(ctypes.byref(s))
-    return HostGraph(m, s.n, rp, ci, val)
+    return HostGraph(m, n, rp, ci, val, symmetric)
 
 
 def load_mtx(path: str, undirected: bool) -> HostGraph:
     s = L.HostCSR()
     L.check(L.lib().apspie_load_mtx(path.encode(), int(undirected), ctypes.byref(s)), None,
             f"load_mtx({path})")
-    return _from_struct(s)
+    return _from_struct(s, symmetric=bool(undirected))
 
 
 def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, weight_seed: int = 3,
@@ -88,7 +90,7 @@ def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, weight_seed: int 
     s = L.HostCSR()
     L.check(L.lib().apspie_gen_rmat(scale, edge_factor, seed, weight_seed, a, b, c, int(weights),
                                     ctypes.byref(s)), None, "gen_rmat")
-    return _from_struct(s)
+    return _from_struct(s, symmetric=True)
 
 
 def gen_er(n: int, k: int = 8, seed: int = 5, val_type: int = L.VAL_F32) -> HostGraph:
@@ -135,14 +137,17 @@ class DeviceGraph:
         self.col_ind = torch.from_numpy(np.ascontiguousarray(g.col_ind, dtype=np.int32)).to(device)
         self.val = None if g.val is None else torch.from_numpy(np.ascontiguousarray(g.val)).to(device)
         self.val_type = g.val_type
+        self.symmetric = bool(g.symmetric)
 
     @classmethod
-    def from_tensors(cls, m: int, n: int, row_ptr, col_ind, val=None, val_type: int = L.VAL_NONE):
+    def from_tensors(cls, m: int, n: int, row_ptr, col_ind, val=None, val_type: int = L.VAL_NONE,
+                     symmetric: bool = False):
         """Wraps existing device tensors (no copy)."""
         self = cls.__new__(cls)
         self.m, self.n, self.nnz = m, n, int(col_ind.shape[0])
         self.row_ptr, self.col_ind, self.val = row_ptr, col_ind, val
         self.val_type = val_type if val is not None else L.VAL_NONE
+        self.symmetric = symmetric
         return self
 
     def view(self, with_values: bool = True) -> L.CSR:
@@ -156,6 +161,8 @@ class DeviceGraph:
         else:
             s.val_type = L.VAL_NONE
             s.val = None
+        s.flags = L.CSR_SYMMETRIC if self.symmetric else 0
+        s.reserved = 0
         return s
 
 
@@ -203,6 +210,12 @@ class Context:
 
     def set_bfs_tuning(self, alpha: float, beta: float) -> None:
         self._check(L.lib().apspie_ctx_set_bfs_tuning(self.handle, alpha, beta), "set_bfs_tuning")
+
+    def set_sssp_delta(self, delta: int) -> None:
+        self._check(L.lib().apspie_ctx_set_sssp_delta(self.handle, delta), "set_sssp_delta")
+
+    def set_max_grid(self, blocks: int) -> None:
+        self._check(L.lib().apspie_ctx_set_max_grid(self.handle, blocks), "set_max_grid")
 
     def reserve(self, m: int, nnz: int) -> None:
         self._check(L.lib().apspie_ctx_reserve(self.handle, m, nnz), "reserve")

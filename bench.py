@@ -71,7 +71,8 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.5)  # let the sampler come up before the timed region
         except Exception:
             self.proc = None
 
@@ -408,7 +409,7 @@ def extras(ctx, args, ws, local):
 def main():
     ap_ = argparse.ArgumentParser()
     ap_.add_argument("--gpus", type=int, default=1)
-    ap_.add_argument("--steps", type=int, default=20)
+    ap_.add_argument("--steps", type=int, default=100)
     ap_.add_argument("--warmup", type=int, default=3)
     ap_.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap_.add_argument("--no-extra", action="store_true")

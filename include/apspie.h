@@ -45,6 +45,14 @@ typedef enum apspie_val_type {
     APSPIE_VAL_I32 = 2
 } apspie_val_type;
 
+/* apspie_csr.flags */
+enum {
+    /* The caller asserts that the pattern is symmetric (an undirected graph, as built by
+     * the reference's makeSymmetric). Enables bottom-up (pull) BFS levels, which scan a
+     * vertex's own row for parents; without it BFS expands top-down only. */
+    APSPIE_CSR_SYMMETRIC = 1u
+};
+
 /* Device-resident CSR matrix view (not owned). */
 typedef struct apspie_csr {
     int32_t m;             /* rows */
@@ -54,6 +62,8 @@ typedef struct apspie_csr {
     const int32_t *row_ptr; /* d, m+1 */
     const int32_t *col_ind; /* d, nnz */
     const void *val;        /* d, nnz elements of val_type, or NULL */
+    uint32_t flags;         /* APSPIE_CSR_* */
+    uint32_t reserved;      /* 0 */
 } apspie_csr;
 
 /* Device-resident CSR matrix allocated by the library (spgemm output); release with
@@ -96,6 +106,12 @@ apspie_status apspie_ctx_set_validate(apspie_ctx *ctx, int on);
 /* Direction-switch thresholds for BFS (Beamer's alpha/beta; defaults 14 and 24).
  * alpha <= 0 forces push on every level. */
 apspie_status apspie_ctx_set_bfs_tuning(apspie_ctx *ctx, float alpha, float beta);
+/* SSSP bucket width (delta-stepping "near/far" threshold step). delta <= 0 (default)
+ * picks it on the device from a sample of the weights: 32 * mean weight / mean degree. */
+apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta);
+/* Caps the number of co-resident blocks of the persistent traversal kernels
+ * (0 = as many as fit). */
+apspie_status apspie_ctx_set_max_grid(apspie_ctx *ctx, int32_t max_blocks);
 /* Bytes of device scratch the context currently holds. */
 int64_t apspie_ctx_scratch_bytes(const apspie_ctx *ctx);
 
@@ -104,14 +120,16 @@ apspie_status apspie_csr_validate(apspie_ctx *ctx, const apspie_csr *A);
 
 /* ---- traversal (SpMSpV) --------------------------------------------------------- */
 
-/* Level-synchronous BFS by boolean OR-AND SpMSpV with a push/pull switch.
+/* Level-synchronous BFS by boolean OR-AND SpMSpV with a push/pull switch (pull only
+ * when A->flags has APSPIE_CSR_SYMMETRIC).
  * d_depth[m] (int32, caller-allocated): hop count from `source`, -1 unreached.
  * Replaces spmspvBfs (src/spmspvBfs.cuh:96) and bfs<T> (src/bfs.cuh:33). */
 apspie_status apspie_bfs(apspie_ctx *ctx, const apspie_csr *A, int32_t source,
                          int32_t depth_cap, int32_t *d_depth, apspie_run_stats *stats);
 
 /* Single-source shortest paths by min-plus SpMSpV over int32 edge weights >= 0
- * (A->val_type == APSPIE_VAL_I32), iterated on the device to the fixed point.
+ * (A->val_type == APSPIE_VAL_I32), iterated on the device to the fixed point with
+ * near/far buckets of width delta (apspie_ctx_set_sssp_delta).
  * d_dist[m] (int32): distance, -1 unreached (the CPU check's convention,
  * src/testSssp.cpp:50). Replaces sssp<Value> (src/sssp.cuh:28) and
  * spmspvSssp (src/spmspvSssp.cuh:92). Returns APSPIE_ERR_INVALID_ARG when a path

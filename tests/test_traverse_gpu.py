@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 def _dev(golden, key, with_w=False):
     rp, ci = golden[key + "_row_ptr"], golden[key + "_col_ind"]
     val = golden[key + "_w"] if with_w else None
-    g = ap.HostGraph(rp.shape[0] - 1, rp.shape[0] - 1, rp, ci, val)
+    g = ap.HostGraph(rp.shape[0] - 1, rp.shape[0] - 1, rp, ci, val, symmetric=key.endswith("_u"))
     return g, ap.DeviceGraph(g)
 
 
@@ -92,7 +92,7 @@ def test_bfs_isolated_source_and_empty_rows(ctx):
     # vertices 0..3 isolated, a path 4-5-6, vertex 7 isolated
     rp = np.array([0, 0, 0, 0, 0, 1, 3, 4, 4], dtype=np.int32)
     ci = np.array([5, 4, 6, 5], dtype=np.int32)
-    g = ap.HostGraph(8, 8, rp, ci)
+    g = ap.HostGraph(8, 8, rp, ci, symmetric=True)
     dg = ap.DeviceGraph(g)
     for s in range(8):
         np.testing.assert_array_equal(ctx.bfs(dg, s).cpu().numpy(), oracle.bfs(rp, ci, s))
@@ -134,7 +134,7 @@ def test_sssp_zero_weights_and_repeated_calls(ctx, rmat14):
     g, _, src = rmat14
     w = g.val.copy()
     w[::3] = 0
-    h = ap.HostGraph(g.m, g.n, g.row_ptr, g.col_ind, w)
+    h = ap.HostGraph(g.m, g.n, g.row_ptr, g.col_ind, w, symmetric=True)
     dg = ap.DeviceGraph(h)
     ref = oracle.sssp(h.row_ptr, h.col_ind, h.val, src)
     for _ in range(3):
@@ -219,7 +219,7 @@ def test_poisoned_csr_caught_by_validation(ctx, rmat14):
     g, _, src = rmat14
     bad = g.col_ind.copy()
     bad[123] = g.m + 5  # column out of range
-    dg = ap.DeviceGraph(ap.HostGraph(g.m, g.n, g.row_ptr, bad, g.val))
+    dg = ap.DeviceGraph(ap.HostGraph(g.m, g.n, g.row_ptr, bad, g.val, symmetric=True))
     with pytest.raises(ap.ApspieError):
         ctx.validate(dg)
     ctx.set_validate(True)
@@ -248,3 +248,43 @@ def test_negative_weight_reported_not_hung(ctx):
     out = torch.empty(2, dtype=torch.int32, device="cuda")
     with pytest.raises(ap.ApspieError):
         ctx.sssp_into(dg, 0, out, stats=True)
+
+
+def test_bfs_directed_graph_never_pulls(ctx, golden):
+    """A directed pattern must be expanded top-down only: pull would follow in-edges."""
+    import torch
+
+    g, dg = _dev(golden, "chesapeake_d")
+    assert not dg.symmetric
+    out = torch.empty(g.m, dtype=torch.int32, device="cuda")
+    for s in range(g.m):
+        st = ctx.bfs_into(dg, s, out, stats=True)
+        assert st["pull_iterations"] == 0
+        np.testing.assert_array_equal(out.cpu().numpy(), golden["chesapeake_d_bfs"][s])
+
+
+@pytest.mark.parametrize("delta", [1, 7, 64, 100000])
+def test_sssp_bucket_width_does_not_change_result(ctx, rmat14, delta):
+    g, dg, src = rmat14
+    ref = oracle.sssp(g.row_ptr, g.col_ind, g.val, src)
+    ctx.set_sssp_delta(delta)
+    try:
+        np.testing.assert_array_equal(ctx.sssp(dg, src).cpu().numpy(), ref)
+    finally:
+        ctx.set_sssp_delta(0)
+
+
+@pytest.mark.parametrize("blocks", [1, 3, 148])
+def test_grid_size_does_not_change_results(ctx, rmat14, blocks):
+    import torch
+
+    g, dg, src = rmat14
+    ctx.set_max_grid(blocks)
+    try:
+        np.testing.assert_array_equal(ctx.bfs(dg, src).cpu().numpy(), oracle.bfs(g.row_ptr, g.col_ind, src))
+        np.testing.assert_array_equal(ctx.sssp(dg, src).cpu().numpy(), oracle.sssp(g.row_ptr, g.col_ind, g.val, src))
+        pr = ap.mt19937_u32(4, g.m)
+        got = ctx.mis(dg, torch.from_numpy(pr.view(np.int32)).cuda()).cpu().numpy()
+        np.testing.assert_array_equal(got, oracle.mis_greedy(g.row_ptr, g.col_ind, pr))
+    finally:
+        ctx.set_max_grid(0)
