@@ -86,6 +86,7 @@ SIGNATURES = {
     "apspie_ctx_set_sssp_delta": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_set_max_grid": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_scratch_bytes": (c_int64, [c_void_p]),
+    "apspie_ctx_timeline": (c_int, [c_void_p, c_void_p, c_void_p, c_int32, POINTER(c_int32)]),
     "apspie_csr_validate": (c_int, [c_void_p, POINTER(CSR)]),
     # traversal
     "apspie_bfs": (c_int, [c_void_p, POINTER(CSR), c_int32, c_int32, c_void_p, POINTER(RunStats)]),

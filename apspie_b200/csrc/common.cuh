@@ -12,6 +12,8 @@
 
 namespace apspie {
 
+constexpr int kTimeline = 128;
+
 // ---------------------------------------------------------------------------------
 // Per-call device control block. Reset by the host (one memset) before each launch.
 // ---------------------------------------------------------------------------------
@@ -30,6 +32,9 @@ struct TravCtl {
     long long edges_component;
     long long vertices_reached;
     long long aux[4];    // kernel-specific counters
+    int tl_count;        // phase timeline: block 0 stamps every grid barrier it passes
+    int tl_site[kTimeline];
+    unsigned long long tl_ns[kTimeline];
 };
 
 // Upper bound on a persistent grid (chunk sums are staged in shared memory).
@@ -73,8 +78,11 @@ apspie_status validate_csr(apspie_ctx *ctx, const apspie_csr *A, bool need_squar
 // Checks host-visible CSR view fields (no device access).
 apspie_status check_csr_view(apspie_ctx *ctx, const apspie_csr *A, const char *who);
 // Cooperative launch of a persistent kernel with the largest co-resident grid.
+// `work` (edges the graph holds) sizes the grid: about one block per kWorkPerBlock edges,
+// at least one per SM, at most the co-resident limit (barrier cost grows with blocks).
+constexpr long long kWorkPerBlock = 4096;
 apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, void **args,
-                                int *grid_out, int max_grid = kMaxGrid);
+                                long long work, int *grid_out = nullptr);
 // Copies the control block back, synchronises, and turns a device error into a status.
 apspie_status finish_call(apspie_ctx *ctx, apspie_run_stats *stats, const char *who);
 
@@ -122,6 +130,18 @@ __device__ __forceinline__ int ld_volatile_i32(const int *p) {
     return *reinterpret_cast<const volatile int *>(p);
 }
 
+// Block 0, thread 0: records (site, globaltimer) in the control block's timeline.
+__device__ __forceinline__ void timeline_mark(TravCtl *ctl, int site) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int k = ctl->tl_count;
+        if (k < kTimeline) {
+            ctl->tl_site[k] = site;
+            ctl->tl_ns[k] = globaltimer_ns();
+            ctl->tl_count = k + 1;
+        }
+    }
+}
+
 __device__ __forceinline__ void raise_error(TravCtl *ctl, int *sticky, int status, int where) {
     if (atomicCAS(&ctl->err, 0, status) == 0) ctl->err_where = where;
     atomicCAS(sticky, 0, status);
@@ -159,6 +179,7 @@ __device__ __forceinline__ bool grid_barrier(TravCtl *ctl, int *sticky, int wher
         __threadfence();
         if (ld_volatile_i32(&ctl->err) != 0) ok = 0;
         s_ok = ok;
+        timeline_mark(ctl, where);
     }
     __syncthreads();
     return s_ok != 0;
@@ -208,6 +229,42 @@ __device__ __forceinline__ void warp_append(bool pred, int v, int *q, int *qlen)
     base = __shfl_sync(0xffffffffu, base, leader);
     if (pred) q[base + __popc(mask & ((1u << lane) - 1u))] = v;
 }
+
+// Per-warp staging buffer for queue appends: entries collect in shared memory and one
+// atomicAdd on the queue length reserves room for up to QCAP of them at a time, instead
+// of one contended global atomic per warp step. `count` is warp-uniform (a register of
+// every lane). All 32 lanes must call push/flush.
+template <int QCAP>
+struct WarpQueue {
+    int *buf;   // shared memory, QCAP entries, private to the warp
+    int *q;     // global queue
+    int *qlen;  // global queue length
+    int count;
+
+    __device__ __forceinline__ WarpQueue(int *b, int *queue, int *len)
+        : buf(b), q(queue), qlen(len), count(0) {}
+
+    __device__ __forceinline__ void flush() {
+        __syncwarp();
+        if (count == 0) return;
+        const int lane = threadIdx.x & 31;
+        int base = 0;
+        if (lane == 0) base = atomicAdd(qlen, count);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        for (int i = lane; i < count; i += 32) q[base + i] = buf[i];
+        __syncwarp();
+        count = 0;
+    }
+
+    __device__ __forceinline__ void push(bool pred, int v) {
+        const unsigned mask = __ballot_sync(0xffffffffu, pred);
+        if (mask == 0) return;
+        if (count + 32 > QCAP) flush();
+        const int lane = threadIdx.x & 31;
+        if (pred) buf[count + __popc(mask & ((1u << lane) - 1u))] = v;
+        count += __popc(mask);
+    }
+};
 
 #endif  // __CUDACC__
 

@@ -115,13 +115,15 @@ apspie_status validate_csr(apspie_ctx *ctx, const apspie_csr *A, bool need_squar
 }
 
 apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, void **args,
-                                int *grid_out, int max_grid) {
+                                long long work, int *grid_out) {
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, block, 0);
     if (e != cudaSuccess) return cuda_error(ctx, e, "occupancy query");
     if (per_sm < 1) return set_error(ctx, APSPIE_ERR_CUDA, "persistent kernel cannot be resident");
     int grid = per_sm * ctx->num_sms;
-    if (grid > max_grid) grid = max_grid;
+    const long long want = (work + kWorkPerBlock - 1) / kWorkPerBlock;
+    if (want < grid) grid = static_cast<int>(want < ctx->num_sms ? ctx->num_sms : want);
+    if (grid > per_sm * ctx->num_sms) grid = per_sm * ctx->num_sms;
     if (ctx->max_grid > 0 && grid > ctx->max_grid) grid = ctx->max_grid;
     if (grid > kMaxGrid) grid = kMaxGrid;
     e = cudaLaunchCooperativeKernel(func, dim3(grid), dim3(block), args, 0, ctx->stream);
@@ -249,6 +251,20 @@ apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta) {
 apspie_status apspie_ctx_set_max_grid(apspie_ctx *ctx, int32_t max_blocks) {
     if (!ctx || max_blocks < 0) return APSPIE_ERR_INVALID_ARG;
     ctx->max_grid = max_blocks;
+    return APSPIE_OK;
+}
+
+apspie_status apspie_ctx_timeline(const apspie_ctx *ctx, int32_t *sites, int64_t *ns, int32_t cap,
+                                  int32_t *count) {
+    if (!ctx || !count || cap < 0 || (cap > 0 && (!sites || !ns))) return APSPIE_ERR_INVALID_ARG;
+    const TravCtl &c = *ctx->h_ctl;
+    int n = c.tl_count < kTimeline ? c.tl_count : kTimeline;
+    if (n > cap) n = cap;
+    for (int i = 0; i < n; ++i) {
+        sites[i] = c.tl_site[i];
+        ns[i] = static_cast<int64_t>(c.tl_ns[i] - c.tl_ns[0]);
+    }
+    *count = n;
     return APSPIE_OK;
 }
 

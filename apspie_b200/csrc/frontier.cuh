@@ -9,32 +9,42 @@
 //           entry's CSR row start and length, and writes a block-local exclusive scan
 //           of the lengths plus one chunk total (no host round trip);
 //  barrier
-//  phase B  every block loads the chunk totals (the second level of the scan), and the
-//           (entries + edges) merge path is cut into tiles of BLOCK*VT items. Each tile
-//           finds its two split points by binary search on the diagonal, stages its
-//           entries' offsets/row starts in shared memory, merges them serially per
-//           thread to label every edge slot with its owning entry, and then visits the
-//           tile's edges strided across the block so that neighbour-index loads of a row
-//           are coalesced. The semiring operation runs on each (entry, edge) pair in the
-//           same pass (no materialised neighbour list, no sort).
+//  phase B  every block loads the chunk totals (the second level of the scan). The merge
+//           path of (frontier entries, edges) is cut into warp tiles of 32*VT items; each
+//           block owns a contiguous run of them. The block finds the split point of every
+//           tile of a batch in parallel (one two-level binary search per thread: chunk
+//           bases in shared memory, then the chunk's local offsets), then each warp walks
+//           its tiles on its own: it stages the tile's entries in its shared-memory slice,
+//           merges them per lane to label every edge slot with its owning entry, and hands
+//           each lane VT edges (strided, so a row's neighbour indices are read coalesced)
+//           whose loads the operation issues back to back. No block barrier inside the
+//           tile loop; the semiring operation runs on every (entry, edge) pair in the same
+//           pass (no materialised neighbour list, no sort).
 #pragma once
 
 #include "common.cuh"
 
 namespace apspie {
 
-constexpr int kSplitBatch = 256;
-
 template <int BLOCK, int VT>
 struct ExpandSmem {
-    static constexpr int NV = BLOCK * VT;
+    static constexpr int NWARP = BLOCK / 32;
+    static constexpr int WT = 32 * VT;  // items (entries + edges) per warp tile
+    static constexpr int BATCH = BLOCK; // warp tiles whose splits are found together
+    struct Warp {
+        int off[WT + 1];   // global edge offset of each staged entry
+        int rs[WT + 1];    // CSR row start of each staged entry
+        int aux[WT + 1];   // per-entry payload (distance snapshot, vertex id, ...)
+        int aux2[WT + 1];  // second payload (priority, ...)
+        int flag[WT + 1];  // per-entry accumulator flushed after the tile
+        int seg[WT];       // tile edge slot -> staged entry
+    };
+    static constexpr int QCAP = 128;  // per-warp queue staging (see WarpQueue)
+    int qbuf[NWARP][2][QCAP];
     int base[kMaxGrid + 1];  // exclusive prefix of chunk totals
-    int off[NV + 1];         // global edge offset of each staged entry
-    int rs[NV + 1];          // CSR row start of each staged entry
-    int aux[NV + 1];         // per-entry payload (vertex id, distance, ...)
-    int seg[NV];             // tile edge slot -> staged entry
+    int tsplit[BATCH + 1];   // merge-path split of each warp tile of the current batch
     int scan_tmp[33];
-    int tsplit[kSplitBatch + 1];  // merge-path split of each tile of the current batch
+    Warp w[NWARP];
 };
 
 // Phase A over this block's chunk of queue q[0, nf). hook(i, v, deg) may rewrite the
@@ -92,75 +102,94 @@ __device__ __forceinline__ int frontier_chunk_bases(const int *__restrict__ chun
 
 // Number of entries among the first `diag` items of the merge of entry offsets
 // (offset(j) = base[j / C] + loc_off[j]) with edge indices 0..E-1, entries first on ties.
+// The first entry of every chunk has loc_off 0, so the search first bisects the chunk
+// starts in shared memory and then at most one chunk's local offsets in global memory.
 __device__ __forceinline__ int frontier_merge_path(long long diag, int nf, int E,
                                                    const int *__restrict__ loc_off,
                                                    const int *base, int C) {
     long long lo = diag - E > 0 ? diag - E : 0;
     long long hi = diag < nf ? diag : nf;
-    while (lo < hi) {
-        const long long mid = (lo + hi) >> 1;
-        const int off = base[mid / C] + __ldcg(loc_off + mid);
-        if (off <= diag - 1 - mid)
-            lo = mid + 1;
-        else
-            hi = mid;
+    if (lo >= hi) return static_cast<int>(lo);
+    long long clo = (lo + C - 1) / C, chi = (hi - 1) / C;
+    while (clo <= chi) {
+        const long long c = (clo + chi) >> 1;
+        if (base[c] <= diag - 1 - c * C) {
+            lo = c * C + 1;
+            clo = c + 1;
+        } else {
+            hi = c * C;
+            chi = c - 1;
+        }
+    }
+    if (lo < hi) {
+        const int cb = base[lo / C];
+        while (lo < hi) {
+            const long long mid = (lo + hi) >> 1;
+            if (cb + __ldcg(loc_off + mid) <= diag - 1 - mid)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
     }
     return static_cast<int>(lo);
 }
 
-// Phase B. load(j, k, sm) stages entry j's payload into sm.aux[k]; op(valid, k, idx, sm)
-// handles the edge at CSR position idx owned by staged entry k. `op` is called by every
-// thread of the block the same number of times (valid=false for idle slots), so it may
-// use warp collectives.
-//
-// Block b owns a contiguous run of tiles. The split points of up to kSplitBatch tiles are
-// found in parallel (one binary search per thread) before the tiles are walked, so the
-// dependent global-memory search latency is paid once per batch rather than per tile.
-template <int BLOCK, int VT, class Load, class Op>
+// Phase B. load(j, k, ws) stages entry j's payload into the warp slice at k;
+// op(valid, k, idx, ws) handles a lane's VT edges (CSR positions idx[], owning staged
+// entries k[]); post(ne, ws) runs after the tile's edges (per-entry flushes). All three
+// are called by every lane of the warp, so they may use warp collectives.
+template <int BLOCK, int VT, class Load, class Op, class Post>
 __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__restrict__ loc_off,
                                                 const int *__restrict__ rs,
-                                                ExpandSmem<BLOCK, VT> &sm, Load load, Op op) {
-    constexpr int NV = BLOCK * VT;
+                                                ExpandSmem<BLOCK, VT> &sm, Load load, Op op,
+                                                Post post) {
+    using S = ExpandSmem<BLOCK, VT>;
+    constexpr int WT = S::WT;
+    constexpr int NWARP = S::NWARP;
+    constexpr int BATCH = S::BATCH;
     const int G = gridDim.x;
     const int C = (nf + G - 1) / G;
     const long long total = static_cast<long long>(nf) + E;
-    const long long ntiles = (total + NV - 1) / NV;
+    const long long ntiles = (total + WT - 1) / WT;
     const long long per = (ntiles + G - 1) / G;
     const long long t_begin = static_cast<long long>(blockIdx.x) * per;
     const long long t_end = t_begin + per < ntiles ? t_begin + per : ntiles;
-    for (long long tb = t_begin; tb < t_end; tb += kSplitBatch) {
-        const long long te = tb + kSplitBatch < t_end ? tb + kSplitBatch : t_end;
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    typename S::Warp &ws = sm.w[wid];
+    for (long long tb = t_begin; tb < t_end; tb += BATCH) {
+        const long long te = tb + BATCH < t_end ? tb + BATCH : t_end;
         for (int s = threadIdx.x; s <= te - tb; s += BLOCK) {
-            long long d = (tb + s) * NV;
+            long long d = (tb + s) * WT;
             if (d > total) d = total;
             sm.tsplit[s] = frontier_merge_path(d, nf, E, loc_off, sm.base, C);
         }
         __syncthreads();
-        for (long long tile = tb; tile < te; ++tile) {
-            const long long d0 = tile * NV;
-            const long long d1 = d0 + NV < total ? d0 + NV : total;
+        for (long long tile = tb + wid; tile < te; tile += NWARP) {
+            const long long d0 = tile * WT;
+            const long long d1 = d0 + WT < total ? d0 + WT : total;
             const int a0 = sm.tsplit[tile - tb];
             const int a1 = sm.tsplit[tile - tb + 1];
             const int e0 = static_cast<int>(d0 - a0);
             const int e1 = static_cast<int>(d1 - a1);
             const int jb = a0 > 0 ? a0 - 1 : 0;
             const int ne = a1 - jb;
-            for (int k = threadIdx.x; k < ne; k += BLOCK) {
+            for (int k = lane; k < ne; k += 32) {
                 const int j = jb + k;
-                sm.off[k] = sm.base[j / C] + __ldcg(loc_off + j);
-                sm.rs[k] = __ldcg(rs + j);
-                load(j, k, sm);
+                ws.off[k] = sm.base[j / C] + __ldcg(loc_off + j);
+                ws.rs[k] = __ldcg(rs + j);
+                load(j, k, ws);
             }
-            __syncthreads();
+            __syncwarp();
             const int tcount = static_cast<int>(d1 - d0);
-            const int diag = threadIdx.x * VT;
+            const int diag = lane * VT;
             if (diag < tcount) {
                 const int acount = a1 - a0, bcount = e1 - e0;
                 int lo = diag - bcount > 0 ? diag - bcount : 0;
                 int hi = diag < acount ? diag : acount;
                 while (lo < hi) {
                     const int mid = (lo + hi) >> 1;
-                    if (sm.off[a0 + mid - jb] <= e0 + diag - 1 - mid)
+                    if (ws.off[a0 + mid - jb] <= e0 + diag - 1 - mid)
                         lo = mid + 1;
                     else
                         hi = mid;
@@ -169,29 +198,36 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
                 int cur = ja - 1 - jb;
                 const int end = diag + VT < tcount ? diag + VT : tcount;
                 for (int it = diag; it < end; ++it) {
-                    if (ja < a1 && sm.off[ja - jb] <= eb) {
+                    if (ja < a1 && ws.off[ja - jb] <= eb) {
                         cur = ja - jb;
                         ++ja;
                     } else {
-                        sm.seg[eb - e0] = cur;
+                        ws.seg[eb - e0] = cur;
                         ++eb;
                     }
                 }
             }
-            __syncthreads();
+            __syncwarp();
             const int ned = e1 - e0;
-            for (int k0 = 0; k0 < ned; k0 += BLOCK) {
-                const int el = k0 + threadIdx.x;
-                const bool valid = el < ned;
-                int k = 0, idx = 0;
-                if (valid) {
-                    k = sm.seg[el];
-                    idx = sm.rs[k] + (e0 + el - sm.off[k]);
+            bool valid[VT];
+            int kk[VT], idx[VT];
+#pragma unroll
+            for (int r = 0; r < VT; ++r) {
+                const int el = r * 32 + lane;
+                valid[r] = el < ned;
+                kk[r] = 0;
+                idx[r] = 0;
+                if (valid[r]) {
+                    kk[r] = ws.seg[el];
+                    idx[r] = ws.rs[kk[r]] + (e0 + el - ws.off[kk[r]]);
                 }
-                op(valid, k, idx, sm);
             }
-            __syncthreads();
+            op(valid, kk, idx, ws);
+            __syncwarp();
+            post(ne, ws);
+            __syncwarp();
         }
+        __syncthreads();
     }
 }
 

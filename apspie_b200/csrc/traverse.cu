@@ -15,9 +15,15 @@ namespace apspie {
 
 namespace {
 
-constexpr int kBlock = 512;
+constexpr int kBlock = 256;
 constexpr int kVT = 4;
 using Smem = ExpandSmem<kBlock, kVT>;
+using WarpSlice = Smem::Warp;
+using WQ = WarpQueue<Smem::QCAP>;
+
+struct NoPost {
+    __device__ void operator()(int, WarpSlice &) const {}
+};
 
 constexpr int kInf = 0x7fffffff;
 
@@ -28,6 +34,10 @@ enum : int {
     kSiteSsspNegWeight = 201,
     kSiteSsspOverflow = 202,
     kSiteSsspIterCap = 203,
+    kSiteSsspBarA = 210,
+    kSiteSsspBarB = 211,
+    kSiteSsspBarF0 = 212,
+    kSiteSsspBarF1 = 213,
     kSiteMis = 300,
     kSiteMisRoundCap = 301,
 };
@@ -91,6 +101,7 @@ struct BfsArgs {
 // frontier holds fewer than m/beta vertices. Depth results do not depend on the choice.
 __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
     __shared__ Smem sm;
+    timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
     const int gtid = blockIdx.x * kBlock + threadIdx.x;
     const int gstride = G * kBlock;
@@ -149,29 +160,37 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
         ++levels;
 
         // phase B
+        const int wid = threadIdx.x >> 5;
+        WQ wq(sm.qbuf[wid][0], qn, qlen_next);
         if (!pull) {
             ++npush;
             const int *col = a.col_ind;
             int *depth = a.depth;
             frontier_expand<kBlock, kVT>(
-                nf, E, a.buf.loc_off, a.buf.rs, sm, [](int, int, Smem &) {},
-                [&](bool valid, int, int idx, Smem &) {
-                    bool fresh = false;
-                    int v = 0;
-                    if (valid) {
-                        v = __ldg(col + idx);
-                        const unsigned bit = 1u << (v & 31);
-                        unsigned *wp = vis + (v >> 5);
-                        if (!(__ldcg(wp) & bit)) {
-                            const unsigned old = atomicOr(wp, bit);
-                            if (!(old & bit)) {
-                                fresh = true;
-                                depth[v] = L;
-                            }
-                        }
+                nf, E, a.buf.loc_off, a.buf.rs, sm, [](int, int, WarpSlice &) {},
+                [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT],
+                    WarpSlice &) {
+                    int v[kVT];
+                    unsigned word[kVT];
+#pragma unroll
+                    for (int r = 0; r < kVT; ++r) v[r] = valid[r] ? __ldg(col + idx[r]) : 0;
+#pragma unroll
+                    for (int r = 0; r < kVT; ++r) word[r] = valid[r] ? __ldcg(vis + (v[r] >> 5)) : ~0u;
+                    bool fresh[kVT];
+#pragma unroll
+                    for (int r = 0; r < kVT; ++r) {
+                        const unsigned bit = 1u << (v[r] & 31);
+                        fresh[r] = false;
+                        if (valid[r] && !(word[r] & bit)) fresh[r] = !(atomicOr(vis + (v[r] >> 5), bit) & bit);
                     }
-                    warp_append(fresh, v, qn, qlen_next);
-                });
+#pragma unroll
+                    for (int r = 0; r < kVT; ++r) {
+                        if (fresh[r]) depth[v[r]] = L;
+                        wq.push(fresh[r], v[r]);
+                    }
+                },
+                NoPost());
+            wq.flush();
         } else {
             ++npull;
             const int lane = threadIdx.x & 31;
@@ -194,9 +213,10 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
                 if (fm) {
                     if (lane == 0) vis[w] = vw | fm;  // this warp owns word w in pull
                     if (found) a.depth[v] = L;
-                    warp_append(found, v, qn, qlen_next);
+                    wq.push(found, v);
                 }
             }
+            wq.flush();
         }
         // the other frontier bitmap is idle this level: clear it for level L+1
         for (int w = gtid; w < words; w += gstride) fbn[w] = 0u;
@@ -242,6 +262,7 @@ struct SsspArgs {
 // the exact fixed point for non-negative integer weights, independent of relaxation order.
 __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     __shared__ Smem sm;
+    timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
     const int gtid = blockIdx.x * kBlock + threadIdx.x;
     const int gstride = G * kBlock;
@@ -308,6 +329,10 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
             const int nfar = ld_volatile_i32(&a.ctl->flen[fc]);
             if (nfar == 0) break;
             thresh += delta;
+            // every block must have read qlen[cur] (== 0) before any block appends to it
+            if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarF0)) return;
+            WQ wn(sm.qbuf[threadIdx.x >> 5][0], qc, &a.ctl->qlen[cur]);
+            WQ wf(sm.qbuf[threadIdx.x >> 5][1], fnext, &a.ctl->flen[fc ^ 1]);
             for (int base = blockIdx.x * kBlock; base < nfar; base += gstride) {
                 const int i = base + threadIdx.x;
                 bool to_near = false, stay = false;
@@ -323,10 +348,12 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                         stay = true;
                     }
                 }
-                warp_append(to_near, v, qc, &a.ctl->qlen[cur]);
-                warp_append(stay, v, fnext, &a.ctl->flen[fc ^ 1]);
+                wn.push(to_near, v);
+                wf.push(stay, v);
             }
-            if (!grid_barrier(a.ctl, a.sticky, kSiteSssp + 3)) return;
+            wn.flush();
+            wf.flush();
+            if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarF1)) return;
             if (gtid == 0) a.ctl->flen[fc] = 0;  // drained; every block read nfar above
             fc ^= 1;
             continue;
@@ -345,7 +372,7 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                                      return deg;
                                  });
         if (gtid == 0) *qlen_next = 0;
-        if (!grid_barrier(a.ctl, a.sticky, kSiteSssp + 1)) return;
+        if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarA)) return;
 
         const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
         expanded += E;
@@ -356,39 +383,63 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
         int *sticky = a.sticky;
         int *flen = &a.ctl->flen[fc];
         const long long T = thresh;
+        WQ wn(sm.qbuf[threadIdx.x >> 5][0], qn, qlen_next);
+        WQ wf(sm.qbuf[threadIdx.x >> 5][1], fcur, flen);
         frontier_expand<kBlock, kVT>(
             nf, E, a.buf.loc_off, a.buf.rs, sm,
-            [&](int j, int k, Smem &s) { s.aux[k] = __ldcg(snap + j); },
-            [&](bool valid, int k, int idx, Smem &s) {
-                bool near = false, far = false;
-                int v = 0;
-                if (valid) {
-                    v = __ldg(col + idx);
-                    const int we = __ldg(wt + idx);
-                    const long long nd = static_cast<long long>(s.aux[k]) + we;
-                    if (we < 0) {
+            [&](int j, int k, WarpSlice &ws) { ws.aux[k] = __ldcg(snap + j); },
+            [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT],
+                WarpSlice &ws) {
+                int v[kVT], we[kVT], cd[kVT], nd[kVT];
+                bool imp[kVT];
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) {
+                    v[r] = valid[r] ? __ldg(col + idx[r]) : 0;
+                    we[r] = valid[r] ? __ldg(wt + idx[r]) : 0;
+                }
+                // plain (L1-cacheable) reads: a stale, larger value only costs an extra atomic
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) cd[r] = valid[r] ? dist[v[r]] : 0;
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) {
+                    imp[r] = false;
+                    nd[r] = 0;
+                    if (!valid[r]) continue;
+                    const long long d = static_cast<long long>(ws.aux[kk[r]]) + we[r];
+                    if (we[r] < 0) {
                         raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSsspNegWeight);
-                    } else if (nd >= kInf) {
+                    } else if (d >= kInf) {
                         raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSsspOverflow);
                     } else {
-                        const int ndi = static_cast<int>(nd);
-                        // a stale (larger) cached value only costs an extra atomic
-                        if (ndi < dist[v]) {
-                            const int old = atomicMin(dist + v, ndi);
-                            if (ndi < old) {
-                                const unsigned bit = 1u << (v & 31);
-                                if (nd < T)
-                                    near = !(atomicOr(inq + (v >> 5), bit) & bit);
-                                else
-                                    far = !(atomicOr(infar + (v >> 5), bit) & bit);
-                            }
-                        }
+                        nd[r] = static_cast<int>(d);
+                        imp[r] = nd[r] < cd[r];
                     }
                 }
-                warp_append(near, v, qn, qlen_next);
-                warp_append(far, v, fcur, flen);
-            });
-        if (!grid_barrier(a.ctl, a.sticky, kSiteSssp + 2)) return;
+                int old[kVT];
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) old[r] = imp[r] ? atomicMin(dist + v[r], nd[r]) : 0;
+                bool near[kVT], far[kVT];
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) {
+                    near[r] = far[r] = false;
+                    if (imp[r] && nd[r] < old[r]) {
+                        const unsigned bit = 1u << (v[r] & 31);
+                        if (nd[r] < T)
+                            near[r] = !(atomicOr(inq + (v[r] >> 5), bit) & bit);
+                        else
+                            far[r] = !(atomicOr(infar + (v[r] >> 5), bit) & bit);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) {
+                    wn.push(near[r], v[r]);
+                    wf.push(far[r], v[r]);
+                }
+            },
+            NoPost());
+        wn.flush();
+        wf.flush();
+        if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarB)) return;
         cur ^= 1;
     }
     // unreached -> -1, and the component statistics
@@ -455,6 +506,7 @@ __device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v)
 // left undecided.
 __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
     __shared__ Smem sm;
+    timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
     const int gtid = blockIdx.x * kBlock + threadIdx.x;
     const int gstride = G * kBlock;
@@ -499,22 +551,49 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         const int r = round;
         frontier_expand<kBlock, kVT>(
             nf, E, a.buf.loc_off, a.buf.rs, sm,
-            [&](int j, int k, Smem &s) { s.aux[k] = __ldcg(qc + j); },
-            [&](bool valid, int k, int idx, Smem &s) {
-                if (!valid) return;
-                const int v = s.aux[k];
-                const int u = __ldg(col + idx);
-                if (u == v) return;
-                const unsigned char su = *reinterpret_cast<volatile unsigned char *>(state + u);
-                if (su == kIn) {
-                    state[v] = kOut;
-                } else if (su == kUndecided && outranks(__ldg(prio + u), u, __ldg(prio + v), v)) {
-                    blocked[v] = r;
+            [&](int j, int k, WarpSlice &ws) {
+                const int v = __ldcg(qc + j);
+                ws.aux[k] = v;
+                ws.aux2[k] = static_cast<int>(__ldg(prio + v));
+                ws.flag[k] = 0;
+            },
+            [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT],
+                WarpSlice &ws) {
+                int u[kVT];
+                unsigned pu[kVT];
+                unsigned char su[kVT];
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) u[r] = valid[r] ? __ldg(col + idx[r]) : 0;
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) {
+                    su[r] = valid[r] ? *reinterpret_cast<volatile unsigned char *>(state + u[r]) : kOut;
+                    pu[r] = valid[r] ? __ldg(prio + u[r]) : 0u;
+                }
+#pragma unroll
+                for (int r = 0; r < kVT; ++r) {
+                    if (!valid[r]) continue;
+                    const int v = ws.aux[kk[r]];
+                    if (u[r] == v) continue;
+                    if (su[r] == kIn)
+                        atomicOr(&ws.flag[kk[r]], 1);
+                    else if (su[r] == kUndecided &&
+                             outranks(pu[r], u[r], static_cast<unsigned>(ws.aux2[kk[r]]), v))
+                        atomicOr(&ws.flag[kk[r]], 2);
+                }
+            },
+            [&](int ne, WarpSlice &ws) {
+                for (int k = threadIdx.x & 31; k < ne; k += 32) {
+                    const int f = ws.flag[k];
+                    if (f & 1)
+                        state[ws.aux[k]] = kOut;
+                    else if (f & 2)
+                        blocked[ws.aux[k]] = r;
                 }
             });
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 2)) return;
 
         // vertex pass
+        WQ wq(sm.qbuf[threadIdx.x >> 5][0], qn, qlen_next);
         for (int base = blockIdx.x * kBlock; base < nf; base += gstride) {
             const int i = base + threadIdx.x;
             bool keep = false;
@@ -529,8 +608,9 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                         keep = true;
                 }
             }
-            warp_append(keep, v, qn, qlen_next);
+            wq.push(keep, v);
         }
+        wq.flush();
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 3)) return;
         cur ^= 1;
     }
@@ -634,7 +714,7 @@ apspie_status apspie_bfs(apspie_ctx *ctx, const apspie_csr *A, int32_t source, i
     a.beta = ctx->bfs_beta;
     a.allow_pull = (A->flags & APSPIE_CSR_SYMMETRIC) ? 1 : 0;
     void *args[] = {&a};
-    st = launch_persistent(ctx, reinterpret_cast<const void *>(bfs_kernel), kBlock, args, nullptr);
+    st = launch_persistent(ctx, reinterpret_cast<const void *>(bfs_kernel), kBlock, args, A->nnz);
     if (st != APSPIE_OK) return st;
     return finish_call(ctx, stats, "apspie_bfs");
 }
@@ -667,7 +747,7 @@ apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source, 
     a.ctl = ctx->d_ctl;
     a.sticky = ctx->d_sticky_err;
     void *args[] = {&a};
-    st = launch_persistent(ctx, reinterpret_cast<const void *>(sssp_kernel), kBlock, args, nullptr);
+    st = launch_persistent(ctx, reinterpret_cast<const void *>(sssp_kernel), kBlock, args, A->nnz);
     if (st != APSPIE_OK) return st;
     return finish_call(ctx, stats, "apspie_sssp");
 }
@@ -700,7 +780,7 @@ apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d
     a.ctl = ctx->d_ctl;
     a.sticky = ctx->d_sticky_err;
     void *args[] = {&a};
-    st = launch_persistent(ctx, reinterpret_cast<const void *>(mis_kernel), kBlock, args, nullptr);
+    st = launch_persistent(ctx, reinterpret_cast<const void *>(mis_kernel), kBlock, args, A->nnz);
     if (st != APSPIE_OK) return st;
     return finish_call(ctx, stats, "apspie_mis");
 }

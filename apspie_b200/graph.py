@@ -220,6 +220,15 @@ class Context:
     def reserve(self, m: int, nnz: int) -> None:
         self._check(L.lib().apspie_ctx_reserve(self.handle, m, nnz), "reserve")
 
+    def timeline(self):
+        """[(site, ns since kernel start)] of the last call made with stats=True."""
+        sites = np.zeros(128, dtype=np.int32)
+        ns = np.zeros(128, dtype=np.int64)
+        n = ctypes.c_int32()
+        self._check(L.lib().apspie_ctx_timeline(self.handle, sites.ctypes.data, ns.ctypes.data, 128,
+                                                ctypes.byref(n)), "timeline")
+        return list(zip(sites[:n.value].tolist(), ns[:n.value].tolist()))
+
     def scratch_bytes(self) -> int:
         return int(L.lib().apspie_ctx_scratch_bytes(self.handle))
 

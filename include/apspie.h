@@ -112,6 +112,11 @@ apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta);
 /* Caps the number of co-resident blocks of the persistent traversal kernels
  * (0 = as many as fit). */
 apspie_status apspie_ctx_set_max_grid(apspie_ctx *ctx, int32_t max_blocks);
+/* Phase timeline of the last traversal call made with a stats pointer: for each grid
+ * barrier block 0 passed (up to 128), the barrier's site code and the nanoseconds since the
+ * kernel started (globaltimer). Site 0 is the kernel start. */
+apspie_status apspie_ctx_timeline(const apspie_ctx *ctx, int32_t *sites, int64_t *ns, int32_t cap,
+                                  int32_t *count);
 /* Bytes of device scratch the context currently holds. */
 int64_t apspie_ctx_scratch_bytes(const apspie_ctx *ctx);
 
