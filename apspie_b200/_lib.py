@@ -93,6 +93,13 @@ SIGNATURES = {
     "apspie_sssp": (c_int, [c_void_p, POINTER(CSR), c_int32, c_void_p, POINTER(RunStats)]),
     "apspie_mis": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p, POINTER(RunStats)]),
     "apspie_spmspv_bool": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p]),
+    # SpGEMM / TC
+    "apspie_spgemm": (c_int, [c_void_p, POINTER(CSR), POINTER(CSR), POINTER(CSROwned)]),
+    "apspie_spgemm_symbolic": (c_int, [c_void_p, POINTER(CSR), POINTER(CSR), c_void_p, POINTER(c_int64)]),
+    "apspie_spgemm_numeric": (c_int, [c_void_p, POINTER(CSR), POINTER(CSR), c_void_p, c_void_p, c_void_p]),
+    "apspie_csr_free": (None, [POINTER(CSROwned)]),
+    "apspie_tc": (c_int, [c_void_p, POINTER(CSR), POINTER(c_int64)]),
+    "apspie_csr_strict_lower_device": (c_int, [c_void_p, POINTER(CSR), POINTER(CSROwned)]),
     # host graph construction
     "apspie_host_csr_free": (None, [POINTER(HostCSR)]),
     "apspie_load_mtx": (c_int, [c_char_p, c_int, POINTER(HostCSR)]),

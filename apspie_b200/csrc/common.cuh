@@ -52,6 +52,9 @@ struct apspie_ctx {
     // scratch arena: one device allocation, carved per call, grown on demand
     void *scratch = nullptr;
     size_t scratch_bytes = 0;
+    // secondary arena for variable-size tables (SpGEMM global tier, ...)
+    void *scratch2 = nullptr;
+    size_t scratch2_bytes = 0;
     // control block (device) + pinned host mirror
     apspie::TravCtl *d_ctl = nullptr;
     apspie::TravCtl *h_ctl = nullptr;
@@ -73,6 +76,7 @@ apspie_status set_error(apspie_ctx *ctx, apspie_status st, const std::string &ms
 apspie_status cuda_error(apspie_ctx *ctx, cudaError_t e, const char *what);
 // Ensures the arena holds `bytes`; returns its base in *out.
 apspie_status scratch_reserve(apspie_ctx *ctx, size_t bytes, void **out);
+apspie_status scratch2_reserve(apspie_ctx *ctx, size_t bytes, void **out);
 // Validates a CSR view on the device (synchronises). Used when ctx->validate is on.
 apspie_status validate_csr(apspie_ctx *ctx, const apspie_csr *A, bool need_square);
 // Checks host-visible CSR view fields (no device access).
@@ -85,6 +89,11 @@ apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, vo
                                 long long work, int *grid_out = nullptr);
 // Copies the control block back, synchronises, and turns a device error into a status.
 apspie_status finish_call(apspie_ctx *ctx, apspie_run_stats *stats, const char *who);
+
+// Device-wide exclusive scan (scan.cu): out[0..n) = prefix of in, out[n] = total.
+size_t scan_scratch_bytes(long long n);
+apspie_status device_exclusive_scan(apspie_ctx *ctx, const int *in, long long n, int *out, void *tmp,
+                                    int *overflow_flag);
 
 // Carves aligned sub-buffers out of the scratch arena.
 struct Carver {

@@ -47,6 +47,23 @@ apspie_status scratch_reserve(apspie_ctx *ctx, size_t bytes, void **out) {
     return APSPIE_OK;
 }
 
+apspie_status scratch2_reserve(apspie_ctx *ctx, size_t bytes, void **out) {
+    if (bytes <= ctx->scratch2_bytes && ctx->scratch2) {
+        *out = ctx->scratch2;
+        return APSPIE_OK;
+    }
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "scratch2_reserve sync");
+    if (ctx->scratch2) cudaFree(ctx->scratch2);
+    ctx->scratch2 = nullptr;
+    ctx->scratch2_bytes = 0;
+    e = cudaMalloc(&ctx->scratch2, bytes);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "scratch2_reserve cudaMalloc");
+    ctx->scratch2_bytes = bytes;
+    *out = ctx->scratch2;
+    return APSPIE_OK;
+}
+
 apspie_status check_csr_view(apspie_ctx *ctx, const apspie_csr *A, const char *who) {
     if (!A) return set_error(ctx, APSPIE_ERR_INVALID_ARG, std::string(who) + ": NULL matrix");
     if (A->m < 0 || A->n < 0 || A->nnz < 0)
@@ -200,6 +217,7 @@ void apspie_ctx_destroy(apspie_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->scratch2) cudaFree(ctx->scratch2);
     if (ctx->d_ctl) cudaFree(ctx->d_ctl);
     if (ctx->d_sticky_err) cudaFree(ctx->d_sticky_err);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
@@ -269,7 +287,7 @@ apspie_status apspie_ctx_timeline(const apspie_ctx *ctx, int32_t *sites, int64_t
 }
 
 int64_t apspie_ctx_scratch_bytes(const apspie_ctx *ctx) {
-    return ctx ? static_cast<int64_t>(ctx->scratch_bytes) : 0;
+    return ctx ? static_cast<int64_t>(ctx->scratch_bytes + ctx->scratch2_bytes) : 0;
 }
 
 apspie_status apspie_csr_validate(apspie_ctx *ctx, const apspie_csr *A) {

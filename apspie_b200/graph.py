@@ -258,6 +258,45 @@ class Context:
         self._check(L.lib().apspie_spmspv_bool(self.handle, ctypes.byref(g.view(False)),
                                                x.data_ptr(), y.data_ptr()), "spmspv_bool")
 
+    # ---- SpGEMM / TC
+    def spgemm(self, A: DeviceGraph, B: DeviceGraph):
+        """C = A*B -> (row_ptr, col_ind, val) numpy arrays (copied back, library memory freed)."""
+        C = L.CSROwned()
+        self._check(L.lib().apspie_spgemm(self.handle, ctypes.byref(A.view(True)), ctypes.byref(B.view(True)),
+                                          ctypes.byref(C)), "spgemm")
+        try:
+            return _owned_to_numpy(C)
+        finally:
+            L.lib().apspie_csr_free(ctypes.byref(C))
+
+    def spgemm_two_step(self, A: DeviceGraph, B: DeviceGraph):
+        """Caller-owned C through apspie_spgemm_symbolic + apspie_spgemm_numeric (torch tensors)."""
+        import torch
+
+        dev = A.row_ptr.device
+        rp = torch.empty(A.m + 1, dtype=torch.int32, device=dev)
+        nnz = ctypes.c_int64()
+        self._check(L.lib().apspie_spgemm_symbolic(self.handle, ctypes.byref(A.view(True)),
+                                                   ctypes.byref(B.view(True)), rp.data_ptr(), ctypes.byref(nnz)),
+                    "spgemm_symbolic")
+        ci = torch.empty(max(nnz.value, 1), dtype=torch.int32, device=dev)
+        vdt = torch.float32 if A.val_type == L.VAL_F32 else torch.int32
+        cv = torch.empty(max(nnz.value, 1), dtype=vdt, device=dev)
+        self._check(L.lib().apspie_spgemm_numeric(self.handle, ctypes.byref(A.view(True)), ctypes.byref(B.view(True)),
+                                                  rp.data_ptr(), ci.data_ptr(), cv.data_ptr()), "spgemm_numeric")
+        return rp, ci[:nnz.value], cv[:nnz.value]
+
+    def tc(self, Lg: DeviceGraph) -> int:
+        out = ctypes.c_int64()
+        self._check(L.lib().apspie_tc(self.handle, ctypes.byref(Lg.view(False)), ctypes.byref(out)), "tc")
+        return int(out.value)
+
+    def strict_lower(self, A: DeviceGraph) -> "OwnedDeviceCSR":
+        C = L.CSROwned()
+        self._check(L.lib().apspie_csr_strict_lower_device(self.handle, ctypes.byref(A.view(False)),
+                                                          ctypes.byref(C)), "strict_lower")
+        return OwnedDeviceCSR(C)
+
     # ---- convenience (allocate outputs)
     def bfs(self, g: DeviceGraph, source: int, depth_cap: int = 0):
         import torch
@@ -279,3 +318,72 @@ class Context:
         out = torch.empty(g.m, dtype=torch.uint8, device=f"cuda:{self.device}")
         self.mis_into(g, prio, out)
         return out
+
+
+def _owned_to_numpy(C: L.CSROwned):
+    import torch
+
+    m, nnz = C.m, C.nnz
+    rp = np.empty(m + 1, dtype=np.int32)
+    ci = np.empty(nnz, dtype=np.int32)
+    val = None
+    ctypes_memcpy_d2h(rp, C.row_ptr)
+    if nnz:
+        ctypes_memcpy_d2h(ci, C.col_ind)
+    if C.val_type == L.VAL_F32:
+        val = np.empty(nnz, dtype=np.float32)
+    elif C.val_type == L.VAL_I32:
+        val = np.empty(nnz, dtype=np.int32)
+    if val is not None and nnz:
+        ctypes_memcpy_d2h(val, C.val)
+    torch.cuda.synchronize()
+    return rp, ci, val
+
+
+class _DeviceArray:
+    """Raw device pointer exposed through __cuda_array_interface__ (no copy)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3}
+
+
+def ctypes_memcpy_d2h(dst: np.ndarray, src_ptr: int) -> None:
+    """Copies a device array (raw pointer) into a numpy array of the same dtype/length."""
+    import torch
+
+    if dst.size == 0:
+        return
+    t = torch.as_tensor(_DeviceArray(src_ptr, dst.size, dst.dtype.str), device="cuda")
+    dst[...] = t.cpu().numpy()
+
+
+class OwnedDeviceCSR:
+    """A library-allocated device CSR (apspie_csr_owned), viewable as a DeviceGraph."""
+
+    def __init__(self, C: L.CSROwned):
+        self.C = C
+        self.m, self.n, self.nnz, self.val_type = C.m, C.n, C.nnz, C.val_type
+        self.symmetric = False
+
+    def view(self, with_values: bool = True) -> L.CSR:
+        s = L.CSR()
+        s.m, s.n, s.nnz = self.m, self.n, self.nnz
+        s.row_ptr, s.col_ind = self.C.row_ptr, self.C.col_ind
+        s.val_type, s.val = (self.val_type, self.C.val) if with_values and self.C.val else (L.VAL_NONE, None)
+        s.flags, s.reserved = 0, 0
+        return s
+
+    def to_numpy(self):
+        return _owned_to_numpy(self.C)
+
+    def free(self):
+        if self.C is not None:
+            L.lib().apspie_csr_free(ctypes.byref(self.C))
+            self.C = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -155,6 +155,35 @@ apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d
 apspie_status apspie_spmspv_bool(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_x,
                                  int32_t *d_y);
 
+/* ---- SpGEMM and triangle counting ---------------------------------------------- */
+
+/* C = A * B, row-binned hash Gustavson. A and B share val_type (F32 or I32). C's rows are
+ * sorted by column; int32 values are exact; FP32 values of rows with at most 128 products
+ * are summed in increasing position of A's row (deterministic), longer rows accumulate by
+ * atomicAdd (summation order only). The library allocates C (release with
+ * apspie_csr_free); synchronises. Replaces spgemm(d_matrix*, d_matrix*, d_matrix*, partSize,
+ * partNum, ctx) (src/spgemm.cuh:132), spgemm<T>(d_matrix*...) (src/spgemm.cuh:346) and
+ * spgemm<T>(edge, m, ..., T*&, int*&, int*&) (src/tc.cuh:63). */
+apspie_status apspie_spgemm(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B,
+                            apspie_csr_owned *C);
+/* Two-step form with caller-owned C: symbolic fills d_row_ptr_c[A->m + 1] and *nnz_c
+ * (synchronises); numeric fills d_col_c[nnz] and d_val_c[nnz] (A's val_type). */
+apspie_status apspie_spgemm_symbolic(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B,
+                                     int32_t *d_row_ptr_c, int64_t *nnz_c);
+apspie_status apspie_spgemm_numeric(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B,
+                                    const int32_t *d_row_ptr_c, int32_t *d_col_c, void *d_val_c);
+void apspie_csr_free(apspie_csr_owned *C);
+
+/* Triangle count = sum((L*L) .* L) for L the strict lower triangle (column < row) of a
+ * symmetric graph, rows sorted; masked hash SpGEMM, L*L never materialised; int64 result
+ * (synchronises). Replaces the flow of test/tc/main.cu:243-249 (spgemm<T> tc.cuh:63 ->
+ * ewiseMultTc tc.cuh:169 -> mgpu::Reduce). */
+apspie_status apspie_tc(apspie_ctx *ctx, const apspie_csr *L, int64_t *count);
+/* Strict lower triangle of a square CSR on the device (buildLower, test/tc/main.cu:39-55,
+ * in CSR); library-allocated, release with apspie_csr_free. Values are dropped. */
+apspie_status apspie_csr_strict_lower_device(apspie_ctx *ctx, const apspie_csr *A,
+                                             apspie_csr_owned *L);
+
 #ifdef __cplusplus
 }
 #endif
