@@ -535,7 +535,9 @@ apspie_status sg_run(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B, 
     Mat a{A->row_ptr, A->col_ind, A->val}, b{B->row_ptr, B->col_ind, B->val};
     const long long mi = static_cast<long long>(m) + 1;
     const int grid_cap = ctx->num_sms * 8;
-    auto rows = [&](int bin) { return p.bin_rows + bin * mi; };
+    (void)mi;
+    // per-bin lists are laid out with stride m (sg_rowinfo)
+    auto rows = [&](int bin) { return p.bin_rows + static_cast<long long>(bin) * m; };
     int nb = p.h.bin_count[1];
     if (nb > 0) {
         const int g = std::min((nb + 7) / 8, grid_cap);

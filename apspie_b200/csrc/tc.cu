@@ -308,13 +308,13 @@ apspie_status apspie_tc(apspie_ctx *ctx, const apspie_csr *L, int64_t *count) {
     const int cap = ctx->num_sms * 8;
     if (h.bin_count[1] > 0)
         tc_warp<<<std::min((h.bin_count[1] + 7) / 8, cap), kTcBlock, 0, ctx->stream>>>(
-            bin_rows + 1 * mi, h.bin_count[1], L->row_ptr, L->col_ind, info);
+            bin_rows + 1 * static_cast<size_t>(m), h.bin_count[1], L->row_ptr, L->col_ind, info);
     if (h.bin_count[2] > 0)
         tc_block<false><<<std::min(h.bin_count[2], cap), kTcBlock, 0, ctx->stream>>>(
-            bin_rows + 2 * mi, h.bin_count[2], L->row_ptr, L->col_ind, tbl_off, gkeys, info);
+            bin_rows + 2 * static_cast<size_t>(m), h.bin_count[2], L->row_ptr, L->col_ind, tbl_off, gkeys, info);
     if (h.bin_count[3] > 0)
         tc_block<true><<<std::min(h.bin_count[3], cap), kTcBlock, 0, ctx->stream>>>(
-            bin_rows + 3 * mi, h.bin_count[3], L->row_ptr, L->col_ind, tbl_off, gkeys, info);
+            bin_rows + 3 * static_cast<size_t>(m), h.bin_count[3], L->row_ptr, L->col_ind, tbl_off, gkeys, info);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "tc launch");
     if ((e = cudaMemcpyAsync(&h, info, sizeof(TcInfo), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
