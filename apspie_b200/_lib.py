@@ -93,6 +93,7 @@ SIGNATURES = {
     "apspie_sssp": (c_int, [c_void_p, POINTER(CSR), c_int32, c_void_p, POINTER(RunStats)]),
     "apspie_mis": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p, POINTER(RunStats)]),
     "apspie_spmspv_bool": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p]),
+    "apspie_bfs_noalloc": (c_int, [POINTER(CSR), c_int32, c_int32, c_void_p, c_void_p, POINTER(RunStats)]),
     # SpGEMM / TC
     "apspie_spgemm": (c_int, [c_void_p, POINTER(CSR), POINTER(CSR), POINTER(CSROwned)]),
     "apspie_spgemm_symbolic": (c_int, [c_void_p, POINTER(CSR), POINTER(CSR), c_void_p, POINTER(c_int64)]),

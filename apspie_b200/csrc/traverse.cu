@@ -8,6 +8,7 @@
 // ~10-14 launches, up to 3 device->host syncs and a cudaMalloc/cudaFree per level, and
 // which stop after a caller-supplied `depth` taken from the CPU BFS.
 #include <cstdio>
+#include <mutex>
 
 #include "frontier.cuh"
 
@@ -668,6 +669,43 @@ apspie_status reset_ctl(apspie_ctx *ctx) {
 
 }  // namespace
 
+// ================================================================================
+// Allocation-free BFS: scratch in a file-scope device array
+// ================================================================================
+namespace {
+
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kNaMaxV = APSPIE_NOALLOC_MAX_VERTICES;
+constexpr size_t kNaQueueBytes = align256((kNaMaxV + 1) * sizeof(int));
+constexpr size_t kNaWordsBytes = align256(((kNaMaxV + 31) / 32) * sizeof(unsigned));
+constexpr size_t kNaCtlBytes = align256(sizeof(TravCtl)) + 256;  // control block + sticky error word
+constexpr size_t kNaBytes =
+    kNaCtlBytes + 4 * kNaQueueBytes + align256(kMaxGrid * sizeof(int)) + 3 * kNaWordsBytes;
+
+// Shared by every apspie_bfs_noalloc call in the process (one copy per device). It keeps
+// the last call's contents; the control block is cleared at the start of each call and the
+// kernel initialises every queue and bitmap it reads.
+static __device__ __align__(256) unsigned char g_bfs_noalloc_scratch[kNaBytes];
+
+constexpr int kNaMaxDevices = 64;
+void *g_na_ptr[kNaMaxDevices] = {};
+std::mutex g_na_mu;
+
+// Device address of g_bfs_noalloc_scratch on the current device, looked up once per device.
+cudaError_t noalloc_scratch(int dev, void **out) {
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    if (!g_na_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_na_ptr[dev] = p;
+    }
+    *out = g_na_ptr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
 apspie_status trav_reserve(apspie_ctx *ctx, int m) {
     void *base;
     return scratch_reserve(ctx, trav_scratch_bytes(m) + static_cast<size_t>(m) * 5 + 512, &base);
@@ -783,6 +821,78 @@ apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d
     st = launch_persistent(ctx, reinterpret_cast<const void *>(mis_kernel), kBlock, args, A->nnz);
     if (st != APSPIE_OK) return st;
     return finish_call(ctx, stats, "apspie_mis");
+}
+
+apspie_status apspie_bfs_noalloc(const apspie_csr *A, int32_t source, int32_t depth_cap, int32_t *d_depth,
+                                 void *cuda_stream, apspie_run_stats *stats) {
+    if (!A || !d_depth || !A->row_ptr || (A->nnz > 0 && !A->col_ind) || A->m != A->n || A->m <= 0 ||
+        A->nnz < 0)
+        return APSPIE_ERR_INVALID_ARG;
+    if (A->m > APSPIE_NOALLOC_MAX_VERTICES) return APSPIE_ERR_INVALID_ARG;  // beyond the static scratch
+    if (source < 0 || source >= A->m) return APSPIE_ERR_INVALID_ARG;
+    cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) return APSPIE_ERR_CUDA;
+    void *base = nullptr;
+    if (noalloc_scratch(dev, &base) != cudaSuccess) return APSPIE_ERR_CUDA;
+    char *p = static_cast<char *>(base);
+    TravCtl *ctl = reinterpret_cast<TravCtl *>(p);
+    int *sticky = reinterpret_cast<int *>(p + align256(sizeof(TravCtl)));
+    p += kNaCtlBytes;
+    BfsArgs a;
+    a.buf.q0 = reinterpret_cast<int *>(p);
+    a.buf.q1 = reinterpret_cast<int *>(p + kNaQueueBytes);
+    a.buf.rs = reinterpret_cast<int *>(p + 2 * kNaQueueBytes);
+    a.buf.loc_off = reinterpret_cast<int *>(p + 3 * kNaQueueBytes);
+    p += 4 * kNaQueueBytes;
+    a.buf.chunk_sum = reinterpret_cast<int *>(p);
+    p += align256(kMaxGrid * sizeof(int));
+    a.buf.bits0 = reinterpret_cast<unsigned *>(p);
+    a.buf.bits1 = reinterpret_cast<unsigned *>(p + kNaWordsBytes);
+    a.buf.bits2 = reinterpret_cast<unsigned *>(p + 2 * kNaWordsBytes);
+    a.buf.q2 = a.buf.q3 = a.buf.aux = a.buf.aux2 = nullptr;  // not used by BFS
+    if (cudaMemsetAsync(ctl, 0, kNaCtlBytes, stream) != cudaSuccess) return APSPIE_ERR_CUDA;
+    a.m = A->m;
+    a.nnz = A->nnz;
+    a.src = source;
+    a.depth_cap = depth_cap;
+    a.row_ptr = A->row_ptr;
+    a.col_ind = A->col_ind;
+    a.depth = d_depth;
+    a.ctl = ctl;
+    a.sticky = sticky;
+    a.alpha = 14.0f;
+    a.beta = 24.0f;
+    a.allow_pull = (A->flags & APSPIE_CSR_SYMMETRIC) ? 1 : 0;
+    int sms = 0, per_sm = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_kernel, kBlock, 0) != cudaSuccess ||
+        per_sm < 1)
+        return APSPIE_ERR_CUDA;
+    long long grid = (static_cast<long long>(A->nnz) + kWorkPerBlock - 1) / kWorkPerBlock;
+    if (grid < sms) grid = sms;
+    if (grid > static_cast<long long>(per_sm) * sms) grid = static_cast<long long>(per_sm) * sms;
+    if (grid > kMaxGrid) grid = kMaxGrid;
+    void *args[] = {&a};
+    if (cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(bfs_kernel), dim3(static_cast<int>(grid)),
+                                    dim3(kBlock), args, 0, stream) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return APSPIE_ERR_CUDA;
+    }
+    TravCtl h;
+    if (cudaMemcpyAsync(&h, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+        return APSPIE_ERR_CUDA;
+    if (stats) {
+        stats->iterations = h.iterations;
+        stats->push_iterations = h.push_iterations;
+        stats->pull_iterations = h.pull_iterations;
+        stats->reserved = 0;
+        stats->edges_expanded = h.edges_expanded;
+        stats->edges_component = h.edges_component;
+        stats->vertices_reached = h.vertices_reached;
+    }
+    return h.err != 0 ? static_cast<apspie_status>(h.err) : APSPIE_OK;
 }
 
 apspie_status apspie_spmspv_bool(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_x,

@@ -149,6 +149,23 @@ apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source,
 apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
                          uint8_t *d_member, apspie_run_stats *stats);
 
+/* BFS that allocates nothing, for callers that cannot call cudaMalloc: code running where
+ * device allocation is forbidden or unavailable (inside another allocator's memory budget,
+ * a host that reserves all device memory up front, a plugin loaded into such a process).
+ * No reference counterpart: the reference has only allocating entry points.
+ * Same semantics and outputs as apspie_bfs, on the CURRENT device and the given stream,
+ * with no context. Its scratch (frontier queues, bitmaps, control block, about 4.3 MB) is a
+ * fixed device array inside the library that every GPU which loads the library holds until
+ * the process exits; graphs above APSPIE_NOALLOC_MAX_VERTICES vertices are rejected with
+ * APSPIE_ERR_INVALID_ARG. The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress), so make that first call before any stream capture. All calls
+ * share the one array: calls that overlap on the GPU (other streams, other host threads)
+ * race and corrupt each other; serialise them. Synchronises `cuda_stream` and returns any
+ * device-side error; `stats` may be NULL. */
+#define APSPIE_NOALLOC_MAX_VERTICES 262144
+apspie_status apspie_bfs_noalloc(const apspie_csr *A, int32_t source, int32_t depth_cap,
+                                 int32_t *d_depth, void *cuda_stream, apspie_run_stats *stats);
+
 /* One-hop boolean SpMSpV y = A^T x over a dense 0/1 int32 vector: d_y[v] = 1 if some
  * u with d_x[u] != 0 has v in its row, else 0. Replaces spmspvCsr
  * (src/spmspvMis.cuh:81), the reference's MIS validity helper. */
