@@ -85,6 +85,7 @@ SIGNATURES = {
     "apspie_ctx_set_bfs_tuning": (c_int, [c_void_p, c_float, c_float]),
     "apspie_ctx_set_sssp_delta": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_set_max_grid": (c_int, [c_void_p, c_int32]),
+    "apspie_ctx_set_batch_push_frac": (c_int, [c_void_p, c_float]),
     "apspie_ctx_scratch_bytes": (c_int64, [c_void_p]),
     "apspie_ctx_timeline": (c_int, [c_void_p, c_void_p, c_void_p, c_int32, POINTER(c_int32)]),
     "apspie_csr_validate": (c_int, [c_void_p, POINTER(CSR)]),
@@ -92,7 +93,11 @@ SIGNATURES = {
     "apspie_bfs": (c_int, [c_void_p, POINTER(CSR), c_int32, c_int32, c_void_p, POINTER(RunStats)]),
     "apspie_sssp": (c_int, [c_void_p, POINTER(CSR), c_int32, c_void_p, POINTER(RunStats)]),
     "apspie_mis": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p, POINTER(RunStats)]),
+    "apspie_sssp_f32": (c_int, [c_void_p, POINTER(CSR), c_int32, c_void_p, c_float, POINTER(RunStats)]),
+    "apspie_mis_int32": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p, POINTER(RunStats)]),
     "apspie_spmspv_bool": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p]),
+    "apspie_bfs_batch": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_int32, c_int32, c_void_p,
+                                 POINTER(RunStats)]),
     "apspie_bfs_noalloc": (c_int, [POINTER(CSR), c_int32, c_int32, c_void_p, c_void_p, POINTER(RunStats)]),
     # SpGEMM / TC
     "apspie_spgemm": (c_int, [c_void_p, POINTER(CSR), POINTER(CSR), POINTER(CSROwned)]),

@@ -65,6 +65,7 @@ struct apspie_ctx {
     float bfs_beta = 24.0f;
     int sssp_delta = 0;  // <= 0: chosen on the device
     int max_grid = 0;    // 0: as many co-resident blocks as fit
+    float batch_push_frac = 0.05f;  // batched BFS: push while frontier edges < frac * nnz
 };
 
 namespace apspie {

@@ -266,6 +266,12 @@ apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta) {
     return APSPIE_OK;
 }
 
+apspie_status apspie_ctx_set_batch_push_frac(apspie_ctx *ctx, float frac) {
+    if (!ctx || !(frac >= 0.0f)) return APSPIE_ERR_INVALID_ARG;
+    ctx->batch_push_frac = frac;
+    return APSPIE_OK;
+}
+
 apspie_status apspie_ctx_set_max_grid(apspie_ctx *ctx, int32_t max_blocks) {
     if (!ctx || max_blocks < 0) return APSPIE_ERR_INVALID_ARG;
     ctx->max_grid = max_blocks;

@@ -8,6 +8,7 @@
 // ~10-14 launches, up to 3 device->host syncs and a cudaMalloc/cudaFree per level, and
 // which stop after a caller-supplied `depth` taken from the CPU BFS.
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 
 #include "frontier.cuh"
@@ -239,6 +240,8 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
 // ================================================================================
 struct SsspArgs {
     int m, nnz, src, delta_hint;
+    int is_float;        // weights/distances are non-negative float32 held as their bit patterns
+    int unreached_bits;  // written for unreached vertices (int -1, or a float's bits)
     const int *__restrict__ row_ptr;
     const int *__restrict__ col_ind;
     const int *__restrict__ w;
@@ -273,8 +276,11 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     unsigned *infar = a.buf.bits1;
     int *last = a.buf.aux2;
 
+    // non-negative float32 values order like their int bit patterns, so one integer
+    // atomicMin serves both weight types; +inf is the float "infinity"
+    const int INF = a.is_float ? 0x7f800000 : kInf;
     for (int i = gtid; i < m; i += gstride) {
-        a.dist[i] = (i == a.src) ? 0 : kInf;
+        a.dist[i] = (i == a.src) ? 0 : INF;
         last[i] = -1;
     }
     for (int w = gtid; w < words; w += gstride) {
@@ -285,13 +291,13 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     constexpr int kSample = 1 << 16;
     const int nsamp = a.nnz < kSample ? a.nnz : kSample;
     if (a.delta_hint <= 0) {
-        long long ws = 0;
-        for (int k = gtid; k < nsamp; k += gstride)
-            ws += __ldg(a.w + static_cast<long long>(k) * a.nnz / nsamp);
+        double ws = 0.0;
+        for (int k = gtid; k < nsamp; k += gstride) {
+            const int wb = __ldg(a.w + static_cast<long long>(k) * a.nnz / nsamp);
+            ws += a.is_float ? static_cast<double>(__int_as_float(wb)) : static_cast<double>(wb);
+        }
         for (int o = 16; o; o >>= 1) ws += __shfl_down_sync(0xffffffffu, ws, o);
-        if ((threadIdx.x & 31) == 0 && ws)
-            atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->aux[0]),
-                      static_cast<unsigned long long>(ws));
+        if ((threadIdx.x & 31) == 0 && ws != 0.0) atomicAdd(reinterpret_cast<double *>(&a.ctl->aux[0]), ws);
     }
     if (gtid == 0) {
         a.buf.q0[0] = a.src;
@@ -302,14 +308,16 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     }
     if (!grid_barrier(a.ctl, a.sticky, kSiteSssp)) return;
 
-    long long delta = a.delta_hint;
+    double delta = a.delta_hint;
     if (delta <= 0) {
-        const double mean_w = nsamp ? static_cast<double>(__ldcg(&a.ctl->aux[0])) / nsamp : 1.0;
+        const double sum = __longlong_as_double(__ldcg(&a.ctl->aux[0]));
+        const double mean_w = nsamp ? sum / nsamp : 1.0;
         const double mean_deg = m ? static_cast<double>(a.nnz) / m : 1.0;
-        delta = static_cast<long long>(32.0 * mean_w / (mean_deg > 1.0 ? mean_deg : 1.0));
-        if (delta < 1) delta = 1;
+        delta = 32.0 * mean_w / (mean_deg > 1.0 ? mean_deg : 1.0);
+        if (!a.is_float) delta = floor(delta);
+        if (!(delta >= 1.0)) delta = a.is_float ? (delta > 0.0 ? delta : 1.0) : 1.0;
     }
-    long long thresh = delta;
+    double thresh = delta;
     int cur = 0, fc = 0;
     long long expanded = 0;
     int iters = 0, steps = 0;
@@ -341,7 +349,8 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                 if (i < nfar) {
                     v = __ldcg(fcur + i);
                     const int d = __ldcg(dist + v);
-                    if (d < thresh) {
+                    const double dv = a.is_float ? static_cast<double>(__int_as_float(d)) : static_cast<double>(d);
+                    if (dv < thresh) {
                         atomicAnd(infar + (v >> 5), ~(1u << (v & 31)));
                         const unsigned bit = 1u << (v & 31);
                         to_near = !(atomicOr(inq + (v >> 5), bit) & bit);
@@ -383,7 +392,8 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
         TravCtl *ctl = a.ctl;
         int *sticky = a.sticky;
         int *flen = &a.ctl->flen[fc];
-        const long long T = thresh;
+        const double T = thresh;
+        const int is_float = a.is_float;
         WQ wn(sm.qbuf[threadIdx.x >> 5][0], qn, qlen_next);
         WQ wf(sm.qbuf[threadIdx.x >> 5][1], fcur, flen);
         frontier_expand<kBlock, kVT>(
@@ -406,6 +416,16 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                     imp[r] = false;
                     nd[r] = 0;
                     if (!valid[r]) continue;
+                    if (is_float) {
+                        const float wf = __int_as_float(we[r]);
+                        if (!(wf >= 0.0f)) {  // negative or NaN
+                            raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSsspNegWeight);
+                        } else {
+                            nd[r] = __float_as_int(__fadd_rn(__int_as_float(ws.aux[kk[r]]), wf));
+                            imp[r] = nd[r] < cd[r];
+                        }
+                        continue;
+                    }
                     const long long d = static_cast<long long>(ws.aux[kk[r]]) + we[r];
                     if (we[r] < 0) {
                         raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSsspNegWeight);
@@ -425,7 +445,9 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                     near[r] = far[r] = false;
                     if (imp[r] && nd[r] < old[r]) {
                         const unsigned bit = 1u << (v[r] & 31);
-                        if (nd[r] < T)
+                        const double ndv = is_float ? static_cast<double>(__int_as_float(nd[r]))
+                                                    : static_cast<double>(nd[r]);
+                        if (ndv < T)
                             near[r] = !(atomicOr(inq + (v[r] >> 5), bit) & bit);
                         else
                             far[r] = !(atomicOr(infar + (v[r] >> 5), bit) & bit);
@@ -447,8 +469,8 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     long long comp = 0, reached = 0;
     for (int i = gtid; i < m; i += gstride) {
         const int d = a.dist[i];
-        if (d == kInf) {
-            a.dist[i] = -1;
+        if (d == INF) {
+            a.dist[i] = a.unreached_bits;
         } else {
             comp += __ldg(a.row_ptr + i + 1) - __ldg(a.row_ptr + i);
             ++reached;
@@ -469,7 +491,7 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
         a.ctl->push_iterations = iters;
         a.ctl->pull_iterations = steps - 1 - iters;  // threshold advances
         a.ctl->edges_expanded = expanded;
-        a.ctl->delta = static_cast<int>(delta);
+        a.ctl->delta = static_cast<int>(delta);  // truncated for float weights
     }
 }
 
@@ -484,6 +506,7 @@ struct MisArgs {
     const int *__restrict__ col_ind;
     const unsigned *__restrict__ prio;
     unsigned char *member;
+    int *member_i32;  // when set, the set is written here as int32 1/0 instead
     unsigned char *state;
     int *blocked;  // round stamp: "an undecided neighbour outranks me in this round"
     TravBuffers buf;
@@ -618,7 +641,10 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
     long long insz = 0;
     for (int i = gtid; i < m; i += gstride) {
         const unsigned char s = a.state[i];
-        a.member[i] = (s == kIn) ? 1 : 0;
+        if (a.member_i32)
+            a.member_i32[i] = (s == kIn) ? 1 : 0;
+        else
+            a.member[i] = (s == kIn) ? 1 : 0;
         insz += (s == kIn);
     }
     for (int o = 16; o; o >>= 1) insz += __shfl_down_sync(0xffffffffu, insz, o);
@@ -757,14 +783,41 @@ apspie_status apspie_bfs(apspie_ctx *ctx, const apspie_csr *A, int32_t source, i
     return finish_call(ctx, stats, "apspie_bfs");
 }
 
+namespace apspie {
+namespace {
+apspie_status sssp_common(apspie_ctx *ctx, const apspie_csr *A, int32_t source, void *d_dist,
+                          apspie_run_stats *stats, bool is_float, int unreached_bits);
+}
+}  // namespace apspie
+
 apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source, int32_t *d_dist,
                           apspie_run_stats *stats) {
     if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    if (A && A->val_type != APSPIE_VAL_I32)
+        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp: int32 edge weights required");
+    return sssp_common(ctx, A, source, d_dist, stats, false, -1);
+}
+
+apspie_status apspie_sssp_f32(apspie_ctx *ctx, const apspie_csr *A, int32_t source, float *d_dist,
+                              float unreached, apspie_run_stats *stats) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    if (A && A->val_type != APSPIE_VAL_F32)
+        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp_f32: float32 edge weights required");
+    int bits;
+    std::memcpy(&bits, &unreached, sizeof bits);
+    return sssp_common(ctx, A, source, d_dist, stats, true, bits);
+}
+
+}  // extern "C"
+
+namespace apspie {
+namespace {
+apspie_status sssp_common(apspie_ctx *ctx, const apspie_csr *A, int32_t source, void *d_dist,
+                          apspie_run_stats *stats, bool is_float, int unreached_bits) {
     cudaSetDevice(ctx->device);
     apspie_status st = prepare_square(ctx, A, "apspie_sssp");
     if (st != APSPIE_OK) return st;
-    if (A->val_type != APSPIE_VAL_I32 || (A->nnz > 0 && !A->val))
-        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp: int32 edge weights required");
+    if (A->nnz > 0 && !A->val) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp: NULL weights");
     if (source < 0 || source >= A->m)
         return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp: source out of range");
     if (!d_dist) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp: NULL output");
@@ -779,8 +832,10 @@ apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source, 
     a.row_ptr = A->row_ptr;
     a.col_ind = A->col_ind;
     a.w = static_cast<const int *>(A->val);
-    a.dist = d_dist;
+    a.dist = static_cast<int *>(d_dist);
     a.delta_hint = ctx->sssp_delta;
+    a.is_float = is_float ? 1 : 0;
+    a.unreached_bits = unreached_bits;
     a.buf = carve_trav(base, A->m);
     a.ctl = ctx->d_ctl;
     a.sticky = ctx->d_sticky_err;
@@ -789,15 +844,34 @@ apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source, 
     if (st != APSPIE_OK) return st;
     return finish_call(ctx, stats, "apspie_sssp");
 }
+}  // namespace
+}  // namespace apspie
+
+extern "C" {
+
+static apspie_status mis_common(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
+                                uint8_t *d_member, int32_t *d_member_i32, apspie_run_stats *stats);
 
 apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
                          uint8_t *d_member, apspie_run_stats *stats) {
     if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    if (!d_member) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_mis: NULL output");
+    return mis_common(ctx, A, d_priority, d_member, nullptr, stats);
+}
+
+apspie_status apspie_mis_int32(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
+                               int32_t *d_mis_result, apspie_run_stats *stats) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    if (!d_mis_result) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_mis_int32: NULL output");
+    return mis_common(ctx, A, d_priority, nullptr, d_mis_result, stats);
+}
+
+static apspie_status mis_common(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
+                                uint8_t *d_member, int32_t *d_member_i32, apspie_run_stats *stats) {
     cudaSetDevice(ctx->device);
     apspie_status st = prepare_square(ctx, A, "apspie_mis");
     if (st != APSPIE_OK) return st;
-    if (!d_priority || !d_member)
-        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_mis: NULL priority or output");
+    if (!d_priority) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_mis: NULL priority");
     void *base;
     const size_t tb = trav_scratch_bytes(A->m);
     const size_t extra = Carver::need({static_cast<size_t>(A->m) * 4, static_cast<size_t>(A->m)});
@@ -811,6 +885,7 @@ apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d
     a.col_ind = A->col_ind;
     a.prio = d_priority;
     a.member = d_member;
+    a.member_i32 = d_member_i32;
     a.buf = carve_trav(base, A->m);
     Carver c(static_cast<char *>(base) + tb);
     a.blocked = c.take<int>(A->m);

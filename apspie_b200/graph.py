@@ -214,6 +214,9 @@ class Context:
     def set_sssp_delta(self, delta: int) -> None:
         self._check(L.lib().apspie_ctx_set_sssp_delta(self.handle, delta), "set_sssp_delta")
 
+    def set_batch_push_frac(self, frac: float) -> None:
+        self._check(L.lib().apspie_ctx_set_batch_push_frac(self.handle, frac), "set_batch_push_frac")
+
     def set_max_grid(self, blocks: int) -> None:
         self._check(L.lib().apspie_ctx_set_max_grid(self.handle, blocks), "set_max_grid")
 
@@ -248,6 +251,18 @@ class Context:
                                         out.data_ptr(), ctypes.byref(st) if st else None), "sssp")
         return st.as_dict() if st else None
 
+    def sssp_f32_into(self, g: DeviceGraph, source: int, out, unreached: float = -1.0, stats: bool = False):
+        st = L.RunStats() if stats else None
+        self._check(L.lib().apspie_sssp_f32(self.handle, ctypes.byref(g.view(True)), source, out.data_ptr(),
+                                            unreached, ctypes.byref(st) if st else None), "sssp_f32")
+        return st.as_dict() if st else None
+
+    def mis_int32_into(self, g: DeviceGraph, prio, out, stats: bool = False):
+        st = L.RunStats() if stats else None
+        self._check(L.lib().apspie_mis_int32(self.handle, ctypes.byref(g.view(False)), prio.data_ptr(),
+                                             out.data_ptr(), ctypes.byref(st) if st else None), "mis_int32")
+        return st.as_dict() if st else None
+
     def mis_into(self, g: DeviceGraph, prio, out, stats: bool = False):
         st = L.RunStats() if stats else None
         self._check(L.lib().apspie_mis(self.handle, ctypes.byref(g.view(False)), prio.data_ptr(),
@@ -257,6 +272,22 @@ class Context:
     def spmspv_bool_into(self, g: DeviceGraph, x, y) -> None:
         self._check(L.lib().apspie_spmspv_bool(self.handle, ctypes.byref(g.view(False)),
                                                x.data_ptr(), y.data_ptr()), "spmspv_bool")
+
+    # ---- batched traversal
+    def bfs_batch_into(self, g: DeviceGraph, sources, out, depth_cap: int = 0, stats: bool = False):
+        """sources: int32 CUDA tensor [nq]; out: int32 CUDA tensor [nq, m] (query-major)."""
+        st = L.RunStats() if stats else None
+        self._check(L.lib().apspie_bfs_batch(self.handle, ctypes.byref(g.view(False)), sources.data_ptr(),
+                                             int(sources.shape[0]), depth_cap, out.data_ptr(),
+                                             ctypes.byref(st) if st else None), "bfs_batch")
+        return st.as_dict() if st else None
+
+    def bfs_batch(self, g: DeviceGraph, sources, depth_cap: int = 0):
+        import torch
+
+        out = torch.empty((int(sources.shape[0]), g.m), dtype=torch.int32, device=f"cuda:{self.device}")
+        self.bfs_batch_into(g, sources, out, depth_cap)
+        return out
 
     # ---- SpGEMM / TC
     def spgemm(self, A: DeviceGraph, B: DeviceGraph):

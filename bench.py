@@ -403,6 +403,84 @@ def extras(ctx, args, ws, local):
     res["bfs_rmat20"] = {"GTEPS": ws * st["edges_component"] / (ms * 1e-3) / 1e9, "ms": ms,
                          "levels": st["iterations"], "push_levels": st["push_iterations"],
                          "pull_levels": st["pull_iterations"]}
+    del d20, o20, mem, prio
+    res.update(extras_spgemm_tc(ctx, args, ws, local))
+    res.update(extras_batched(ctx, args, ws, local))
+    return res
+
+
+def extras_spgemm_tc(ctx, args, ws, local):
+    """C = A*A on ER n=2^20, 8 nnz/row (seed 5), f32 and i32; TC on R-MAT scale 18 (seed 1)."""
+    import torch
+
+    import apspie_b200 as ap
+    import oracle
+
+    res = {}
+    peak, _ = hbm_peak()
+    for vt, tag in ((ap.VAL_F32, "f32"), (ap.VAL_I32, "i32")):
+        e = ap.gen_er(1 << 20, 8, 5, vt)
+        A = ap.DeviceGraph(e, f"cuda:{local}")
+        for _ in range(2):
+            rp, ci, cv = ctx.spgemm_two_step(A, A)
+        steps = 5
+        tot, _ = time_steps(ctx.stream, lambda: ctx.spgemm_two_step(A, A), steps)
+        ms = max_over_ranks(ws, tot / steps)
+        nnz = int(ci.shape[0])
+        alg = (4 * (e.m + 1) + 8 * e.nnz) + (4 * (e.m + 1) + 8 * nnz)
+        orp, oci, ocv = oracle.spgemm(e.m, e.n, e.row_ptr, e.col_ind, e.val, e.row_ptr, e.col_ind, e.val)
+        exact = (np.array_equal(rp.cpu().numpy(), orp) and np.array_equal(ci.cpu().numpy(), oci)
+                 and np.array_equal(cv.cpu().numpy(), ocv))
+        res[f"spgemm_er20_{tag}"] = {"ms": ms, "nnz_C": nnz, "products": 64 * e.m, "alg_GBps": alg / (ms * 1e-3) / 1e9,
+                                     "frac_of_hbm": alg / (ms * 1e-3) / 1e9 / peak, "exact": bool(exact),
+                                     "note": "symbolic + numeric into caller-owned C, two host syncs per call"}
+        del A, rp, ci, cv
+    g = ap.gen_rmat(18, 16, 1, 3, weights=False)
+    Lh = ap.strict_lower(g)
+    Ld = ap.DeviceGraph(Lh, f"cuda:{local}")
+    for _ in range(2):
+        count = ctx.tc(Ld)
+    steps = 5
+    tot, _ = time_steps(ctx.stream, lambda: ctx.tc(Ld), steps)
+    ms = max_over_ranks(ws, tot / steps)
+    wedges = int(np.diff(Lh.row_ptr)[Lh.col_ind].sum())
+    alg = 4 * (Lh.m + 1) + 4 * Lh.nnz + 4 * wedges
+    res["tc_rmat18"] = {"ms": ms, "triangles": count, "nnz_L": Lh.nnz, "wedges": wedges,
+                        "alg_GBps": alg / (ms * 1e-3) / 1e9, "frac_of_hbm": alg / (ms * 1e-3) / 1e9 / peak,
+                        "exact": bool(count == oracle.tc(Lh.row_ptr, Lh.col_ind))}
+    return res
+
+
+def extras_batched(ctx, args, ws, local):
+    """Batched BFS on R-MAT scale 22 (seed 1): batches of 32/128/512 LCC sources (seed 6)
+    against the plain path looping one source at a time over the same sources."""
+    import torch
+
+    import apspie_b200 as ap
+    import oracle
+
+    dev = f"cuda:{local}"
+    g = ap.gen_rmat(22, 16, 1, 3, weights=False)
+    dg = ap.DeviceGraph(g, dev)
+    srcs = ap.lcc_sample(g, 512, 6)
+    one = torch.empty(g.m, dtype=torch.int32, device=dev)
+    for x in srcs[:3]:
+        ctx.bfs_into(dg, int(x), one)
+    tot, _ = time_steps(ctx.stream, lambda: [ctx.bfs_into(dg, int(x), one) for x in srcs[:64]], 1)
+    plain_ms = max_over_ranks(ws, tot / 64)
+    res = {"plain_bfs_rmat22": {"ms_per_query": plain_ms, "queries_per_s": ws * 1e3 / plain_ms}}
+    for nq in (32, 128, 512):
+        s = torch.from_numpy(srcs[:nq]).to(dev)
+        out = torch.empty((nq, g.m), dtype=torch.int32, device=dev)
+        ctx.bfs_batch_into(dg, s, out)
+        tot, per = time_steps(ctx.stream, lambda: ctx.bfs_batch_into(dg, s, out), 3)
+        ms = max_over_ranks(ws, tot / 3)
+        exact = all(np.array_equal(out[q].cpu().numpy(), oracle.bfs(g.row_ptr, g.col_ind, int(srcs[q])))
+                    for q in (0, nq - 1))
+        res[f"batched_bfs_rmat22_B{nq}"] = {"ms_per_batch": ms, "queries_per_s": ws * nq * 1e3 / ms,
+                                            "x_plain": plain_ms * nq / ms, "p99_ms": float(np.percentile(per, 99)),
+                                            "exact_checked_rows": bool(exact)}
+        del out
     return res
 
 

@@ -109,6 +109,9 @@ apspie_status apspie_ctx_set_bfs_tuning(apspie_ctx *ctx, float alpha, float beta
 /* SSSP bucket width (delta-stepping "near/far" threshold step). delta <= 0 (default)
  * picks it on the device from a sample of the weights: 32 * mean weight / mean degree. */
 apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta);
+/* Batched BFS direction switch: a level expands top-down while (active vertices x mean
+ * degree) < frac * nnz, else bottom-up (default 0.05; bottom-up only on symmetric graphs). */
+apspie_status apspie_ctx_set_batch_push_frac(apspie_ctx *ctx, float frac);
 /* Caps the number of co-resident blocks of the persistent traversal kernels
  * (0 = as many as fit). */
 apspie_status apspie_ctx_set_max_grid(apspie_ctx *ctx, int32_t max_blocks);
@@ -149,6 +152,14 @@ apspie_status apspie_sssp(apspie_ctx *ctx, const apspie_csr *A, int32_t source,
 apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
                          uint8_t *d_member, apspie_run_stats *stats);
 
+/* Batched multi-source BFS: num_sources queries on one resident graph, up to 512 per
+ * persistent launch (query-bit SpMSpM levels, push/pull by frontier size). d_depths is
+ * num_sources x m int32, query-major (row q = the depth vector apspie_bfs returns for
+ * d_sources[q]); -1 unreached. Sources may repeat. */
+apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources,
+                               int32_t num_sources, int32_t depth_cap, int32_t *d_depths,
+                               apspie_run_stats *stats);
+
 /* BFS that allocates nothing, for callers that cannot call cudaMalloc: code running where
  * device allocation is forbidden or unavailable (inside another allocator's memory budget,
  * a host that reserves all device memory up front, a plugin loaded into such a process).
@@ -165,6 +176,19 @@ apspie_status apspie_mis(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d
 #define APSPIE_NOALLOC_MAX_VERTICES 262144
 apspie_status apspie_bfs_noalloc(const apspie_csr *A, int32_t source, int32_t depth_cap,
                                  int32_t *d_depth, void *cuda_stream, apspie_run_stats *stats);
+
+/* apspie_sssp over float32 weights >= 0 (A->val_type == APSPIE_VAL_F32): float32
+ * distances, each the fixed point min over paths of float sums (independent of the order
+ * relaxations land, as the reference's CPU ssspCPU computes it); unreached vertices get
+ * `unreached` (the reference GPU path leaves 1.70141e+38, src/sssp.cuh:48; its CPU check
+ * uses -1, src/testSssp.cpp:50). */
+apspie_status apspie_sssp_f32(apspie_ctx *ctx, const apspie_csr *A, int32_t source, float *d_dist,
+                              float unreached, apspie_run_stats *stats);
+
+/* apspie_mis writing the reference's int32 result layout (1 in the set, 0 not;
+ * d_misResult of spmspvMis, src/spmspvMis.cuh:150). */
+apspie_status apspie_mis_int32(apspie_ctx *ctx, const apspie_csr *A, const uint32_t *d_priority,
+                               int32_t *d_mis_result, apspie_run_stats *stats);
 
 /* One-hop boolean SpMSpV y = A^T x over a dense 0/1 int32 vector: d_y[v] = 1 if some
  * u with d_x[u] != 0 has v in its row, else 0. Replaces spmspvCsr

@@ -206,6 +206,17 @@ def ref_sssp(row_ptr, col_ind, weights, source):
     return _ref_vertex_cmd("sssp", row_ptr, col_ind, _i32(weights), source)
 
 
+def ref_sssp_f32(row_ptr, col_ind, weights_f32, source):
+    """ssspCPU on float32 weights; float32 distances (-1 unreached). Returns (dist, info)."""
+    with tempfile.TemporaryDirectory() as d:
+        g = os.path.join(d, "g.csr")
+        out = os.path.join(d, "out.bin")
+        _write_csr(g, row_ptr, col_ind, np.ascontiguousarray(weights_f32, dtype=np.float32))
+        info = _run_ref(["ssspf", g, int(source), out])
+        res = np.fromfile(out, dtype=np.float32)
+    return res, info
+
+
 def ref_mis_vertex_order(row_ptr, col_ind, source=0):
     """misCPU (test/mis/main.cu:90). Returns (set 1/0, info)."""
     return _ref_vertex_cmd("mis", row_ptr, col_ind, None, source)

@@ -10,6 +10,7 @@
 //   apspie_ref load  <file.mtx> <undirected 0|1> <out.csr>
 //   apspie_ref bfs   <in.csr> <source> <out.i32>        (bfsCPU, stop = 1<<30)
 //   apspie_ref sssp  <in.csr> <source> <out.i32>        (ssspCPU on float(weight))
+//   apspie_ref ssspf <in.csr f32> <source> <out.f32>    (ssspCPU, float distances)
 //   apspie_ref mis   <in.csr> <source> <out.i32>        (misCPU, vertex order)
 //   apspie_ref mischeck <in.csr> <member.u8>            (one-hop + uncompareResults)
 //   apspie_ref mt    <seed> <count> <out.u32>           (init_genrand + genrand_int32)
@@ -137,6 +138,21 @@ int main(int argc, char **argv) {
         std::fwrite(g.vf.data(), sizeof(float), g.nnz, f);
         std::fclose(f);
         std::printf("APSPIE_REF {\"cmd\": \"load\", \"m\": %d, \"nnz\": %d}\n", g.m, g.nnz);
+        return 0;
+    }
+    if (cmd == "ssspf" && argc == 5) {  // ssspCPU on float weights, float distances out
+        Csr g;
+        if (!read_csr(argv[2], g)) return 3;
+        const int src = std::atoi(argv[3]);
+        if (src < 0 || src >= g.m || g.vt != 1) return 4;
+        std::vector<float> w(std::max(g.nnz, g.m) + 1, 1.0f);
+        for (int e = 0; e < g.nnz; ++e) w[e] = g.vf[e];
+        std::vector<float> d(g.m);
+        auto t0 = std::chrono::steady_clock::now();
+        ssspCPU(src, g.m, g.rp.data(), g.ci.data(), w.data(), d.data(), 1 << 30);
+        const double ms = ms_since(t0);
+        if (!write_array(argv[4], d.data(), d.size())) return 3;
+        std::printf("APSPIE_REF {\"cmd\": \"ssspf\", \"ms\": %.6f, \"m\": %d, \"nnz\": %d}\n", ms, g.m, g.nnz);
         return 0;
     }
     if ((cmd == "bfs" || cmd == "sssp" || cmd == "mis") && argc == 5) {

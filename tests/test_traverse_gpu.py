@@ -288,3 +288,57 @@ def test_grid_size_does_not_change_results(ctx, rmat14, blocks):
         np.testing.assert_array_equal(got, oracle.mis_greedy(g.row_ptr, g.col_ind, pr))
     finally:
         ctx.set_max_grid(0)
+
+
+# ------------------------------------------------------------ float SSSP / int32 MIS
+def test_sssp_f32_integral_weights_match_golden(ctx, golden):
+    import torch
+
+    for key in ("chesapeake_u", "test_mesh_u", "test_cc_u"):
+        rp, ci = golden[key + "_row_ptr"], golden[key + "_col_ind"]
+        w = golden[key + "_w"].astype(np.float32)
+        dg = ap.DeviceGraph(ap.HostGraph(rp.shape[0] - 1, rp.shape[0] - 1, rp, ci, w, True))
+        out = torch.empty(rp.shape[0] - 1, dtype=torch.float32, device="cuda")
+        for s in range(rp.shape[0] - 1):
+            ctx.sssp_f32_into(dg, s, out, unreached=-1.0)
+            np.testing.assert_array_equal(out.cpu().numpy(), golden[key + "_sssp"][s].astype(np.float32))
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference CPU driver not built")
+def test_sssp_f32_fractional_weights_match_reference_ssspCPU(ctx, rmat14):
+    """Non-integral float weights: the fixed point of float min-plus relaxation does not
+    depend on the order relaxations land, so the GPU result equals the reference's own
+    ssspCPU (label-correcting priority queue, src/testSssp.cpp:33-115) bit for bit."""
+    import torch
+
+    g, _, src = rmat14
+    rows = np.repeat(np.arange(g.m), np.diff(g.row_ptr))
+    lo, hi = np.minimum(rows, g.col_ind), np.maximum(rows, g.col_ind)
+    w = (((lo * 7919 + hi * 104729) % 1000) / 97.0 + 0.01).astype(np.float32)  # symmetric
+    dg = ap.DeviceGraph(ap.HostGraph(g.m, g.n, g.row_ptr, g.col_ind, w, True))
+    out = torch.empty(g.m, dtype=torch.float32, device="cuda")
+    ctx.sssp_f32_into(dg, src, out, unreached=-1.0)
+    ref, _ = oracle.ref_sssp_f32(g.row_ptr, g.col_ind, w, src)
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
+
+
+def test_sssp_f32_unreached_value(ctx):
+    import torch
+
+    rp = np.array([0, 1, 2, 2], dtype=np.int32)
+    ci = np.array([1, 0], dtype=np.int32)
+    w = np.array([0.5, 0.5], dtype=np.float32)
+    dg = ap.DeviceGraph(ap.HostGraph(3, 3, rp, ci, w, True))
+    out = torch.empty(3, dtype=torch.float32, device="cuda")
+    ctx.sssp_f32_into(dg, 0, out, unreached=1.70141e38)
+    np.testing.assert_array_equal(out.cpu().numpy(), np.array([0.0, 0.5, 1.70141e38], dtype=np.float32))
+
+
+def test_mis_int32_layout(ctx, rmat14):
+    import torch
+
+    g, dg, _ = rmat14
+    pr = ap.mt19937_u32(4, g.m)
+    out = torch.empty(g.m, dtype=torch.int32, device="cuda")
+    ctx.mis_int32_into(dg, torch.from_numpy(pr.view(np.int32)).cuda(), out)
+    np.testing.assert_array_equal(out.cpu().numpy(), oracle.mis_greedy(g.row_ptr, g.col_ind, pr).astype(np.int32))
