@@ -8,6 +8,7 @@ from .graph import (
     Context,
     DeviceGraph,
     HostGraph,
+    Server,
     gen_er,
     gen_rmat,
     lcc_sample,
@@ -19,6 +20,6 @@ from .graph import (
 
 __all__ = [
     "ApspieError", "ApspieLibraryMissing", "LIB_PATH", "VAL_F32", "VAL_I32", "VAL_NONE", "lib",
-    "Context", "DeviceGraph", "HostGraph", "gen_er", "gen_rmat", "lcc_sample", "load_mtx",
+    "Context", "DeviceGraph", "HostGraph", "Server", "gen_er", "gen_rmat", "lcc_sample", "load_mtx",
     "max_degree_vertex", "mt19937_u32", "strict_lower",
 ]

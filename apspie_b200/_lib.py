@@ -73,6 +73,16 @@ class RunStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, c_int64) for n in ("submitted", "completed", "failed", "launches", "batched_queries",
+                                        "max_batch_seen", "deferred", "peak_bytes", "resident_bytes")]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+QUERY_BFS, QUERY_SSSP, QUERY_MIS = 0, 1, 2
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     # context
@@ -106,6 +116,15 @@ SIGNATURES = {
     "apspie_csr_free": (None, [POINTER(CSROwned)]),
     "apspie_tc": (c_int, [c_void_p, POINTER(CSR), POINTER(c_int64)]),
     "apspie_csr_strict_lower_device": (c_int, [c_void_p, POINTER(CSR), POINTER(CSROwned)]),
+    # server
+    "apspie_server_create": (c_int, [c_int, c_int64, c_int32, c_int32, POINTER(c_void_p)]),
+    "apspie_server_add_graph": (c_int, [c_void_p, POINTER(HostCSR), c_int32, c_uint32, POINTER(c_int32)]),
+    "apspie_server_start": (c_int, [c_void_p]),
+    "apspie_server_submit": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, POINTER(ctypes.c_uint64)]),
+    "apspie_server_wait": (c_int, [c_void_p, ctypes.c_uint64, c_int32, POINTER(c_double)]),
+    "apspie_server_poll": (c_int, [c_void_p, ctypes.c_uint64, POINTER(c_int32)]),
+    "apspie_server_get_stats": (c_int, [c_void_p, POINTER(ServerStats)]),
+    "apspie_server_destroy": (None, [c_void_p]),
     # host graph construction
     "apspie_host_csr_free": (None, [POINTER(HostCSR)]),
     "apspie_load_mtx": (c_int, [c_char_p, c_int, POINTER(HostCSR)]),

@@ -91,6 +91,11 @@ apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, vo
 // Copies the control block back, synchronises, and turns a device error into a status.
 apspie_status finish_call(apspie_ctx *ctx, apspie_run_stats *stats, const char *who);
 
+// Scratch bytes the entry points reserve in a context's arena (for admission control).
+size_t traversal_scratch_need(int m);        // apspie_bfs / apspie_sssp
+size_t mis_scratch_need(int m);              // apspie_mis
+size_t bfs_batch_scratch_need(int m, int nq);  // apspie_bfs_batch (nq <= 512 per launch)
+
 // Device-wide exclusive scan (scan.cu): out[0..n) = prefix of in, out[n] = total.
 size_t scan_scratch_bytes(long long n);
 apspie_status device_exclusive_scan(apspie_ctx *ctx, const int *in, long long n, int *out, void *tmp,

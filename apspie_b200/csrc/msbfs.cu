@@ -389,7 +389,23 @@ const void *msbfs_fn() {
     return reinterpret_cast<const void *>(msbfs_kernel<W>);
 }
 
+size_t batch_need(int m, int Wp) {
+    const size_t mi = static_cast<size_t>(m) + 1;
+    const size_t mw = static_cast<size_t>(m) * Wp;
+    const size_t words = (static_cast<size_t>(m) + 31) / 32;
+    return Carver::need({mw * 4, mw * 4, mw * 4, words * 4, mi * 4, mi * 4, mi * 4, mi * 4, mi * 4, mi * 4, mi * 4,
+                         kMaxGrid * 4});
+}
+
+int padded_words(int nq) {
+    const int W = (nq + 31) / 32;
+    return W <= 1 ? 1 : W <= 2 ? 2 : W <= 4 ? 4 : W <= 8 ? 8 : 16;
+}
+
 }  // namespace
+
+size_t bfs_batch_scratch_need(int m, int nq) { return batch_need(m, padded_words(nq < 512 ? nq : 512)); }
+
 }  // namespace apspie
 
 using namespace apspie;
@@ -411,16 +427,12 @@ extern "C" apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, 
     if (stats) std::memset(stats, 0, sizeof(*stats));
     for (int q0 = 0; q0 < num_sources; q0 += kMaxQ) {
         const int nq = std::min(kMaxQ, num_sources - q0);
-        const int W = (nq + 31) / 32;
-        const int Wp = W <= 1 ? 1 : W <= 2 ? 2 : W <= 4 ? 4 : W <= 8 ? 8 : 16;
+        const int Wp = padded_words(nq);
         const size_t mi = static_cast<size_t>(m) + 1;
         const size_t mw = static_cast<size_t>(m) * Wp;
         const size_t words = (static_cast<size_t>(m) + 31) / 32;
         void *base;
-        st = scratch_reserve(ctx,
-                             Carver::need({mw * 4, mw * 4, mw * 4, words * 4, mi * 4, mi * 4, mi * 4, mi * 4,
-                                           mi * 4, mi * 4, mi * 4, kMaxGrid * 4}),
-                             &base);
+        st = scratch_reserve(ctx, batch_need(m, Wp), &base);
         if (st != APSPIE_OK) return st;
         Carver c(base);
         MsArgs a;

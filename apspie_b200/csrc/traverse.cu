@@ -732,6 +732,12 @@ cudaError_t noalloc_scratch(int dev, void **out) {
 
 }  // namespace
 
+size_t traversal_scratch_need(int m) { return trav_scratch_bytes(m); }
+
+size_t mis_scratch_need(int m) {
+    return trav_scratch_bytes(m) + Carver::need({static_cast<size_t>(m) * 4, static_cast<size_t>(m)});
+}
+
 apspie_status trav_reserve(apspie_ctx *ctx, int m) {
     void *base;
     return scratch_reserve(ctx, trav_scratch_bytes(m) + static_cast<size_t>(m) * 5 + 512, &base);

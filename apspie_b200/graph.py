@@ -418,3 +418,63 @@ class OwnedDeviceCSR:
             self.free()
         except Exception:
             pass
+
+
+class Server:
+    """apspie_server: HBM-resident graphs, budgeted admission, continuous batching."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 40 << 30, slots: int = 2, max_batch: int = 512):
+        h = ctypes.c_void_p()
+        L.check(L.lib().apspie_server_create(device, budget_bytes, slots, max_batch, ctypes.byref(h)), None,
+                "server_create")
+        self.handle = h
+        self.graphs = []
+
+    def add_graph(self, g: HostGraph, mis_seed: int = 4) -> int:
+        s = g.to_host_struct()
+        if g.val is not None and g.val.dtype == np.int32:
+            self._w = getattr(self, "_w", [])
+            w = np.ascontiguousarray(g.val, dtype=np.int32)
+            self._w.append(w)
+            s.val_type = L.VAL_I32
+            s.val = w.ctypes.data
+        gid = ctypes.c_int32()
+        L.check(L.lib().apspie_server_add_graph(self.handle, ctypes.byref(s), int(g.symmetric), mis_seed,
+                                                ctypes.byref(gid)), None, "server_add_graph")
+        self.graphs.append(g)
+        return gid.value
+
+    def start(self) -> None:
+        L.check(L.lib().apspie_server_start(self.handle), None, "server_start")
+
+    def submit(self, graph_id: int, kind: int, source: int, out) -> int:
+        t = ctypes.c_uint64()
+        L.check(L.lib().apspie_server_submit(self.handle, graph_id, kind, source, out.data_ptr(), ctypes.byref(t)),
+                None, "server_submit")
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 600000) -> float:
+        lat = ctypes.c_double()
+        L.check(L.lib().apspie_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(lat)), None, "server_wait")
+        return lat.value
+
+    def done(self, ticket: int) -> bool:
+        d = ctypes.c_int32()
+        L.check(L.lib().apspie_server_poll(self.handle, ticket, ctypes.byref(d)), None, "server_poll")
+        return bool(d.value)
+
+    def stats(self) -> dict:
+        st = L.ServerStats()
+        L.check(L.lib().apspie_server_get_stats(self.handle, ctypes.byref(st)), None, "server_stats")
+        return st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            L.lib().apspie_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,73 @@
+/*
+ * apspie_server.h -- query server over HBM-resident graphs (continuous batching).
+ *
+ * No reference counterpart: the reference answers one query per process run
+ * (test/bfs/run.sh, test/sssp/run.sh, test/mis/run.sh). The server keeps several graphs on
+ * one GPU, admits BFS / SSSP / MIS requests against a device-memory budget and folds
+ * requests that wait on the same graph into one launch (BFS: apspie_bfs_batch; MIS: one
+ * apspie_mis shared by all waiting requests; SSSP: apspie_sssp per request), on several
+ * execution slots whose launches overlap on the device. Each answer is written by the same
+ * kernels as the plain entry points, so it is identical alone or in a mix.
+ */
+#ifndef APSPIE_SERVER_H
+#define APSPIE_SERVER_H
+
+#include <stdint.h>
+
+#include "apspie.h"
+#include "apspie_host.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    APSPIE_QUERY_BFS = 0,  /* d_out: int32[m] depths (-1 unreached) */
+    APSPIE_QUERY_SSSP = 1, /* d_out: int32[m] distances (-1 unreached); graph needs int32 weights */
+    APSPIE_QUERY_MIS = 2   /* d_out: uint8[m] membership; source ignored */
+};
+
+typedef struct apspie_server apspie_server;
+
+typedef struct apspie_server_stats {
+    int64_t submitted;
+    int64_t completed;
+    int64_t failed;
+    int64_t launches;         /* kernel launches (batches) issued */
+    int64_t batched_queries;  /* requests served by those launches */
+    int64_t max_batch_seen;
+    int64_t deferred;         /* admission attempts postponed by the memory budget */
+    int64_t peak_bytes;       /* largest device footprint admitted */
+    int64_t resident_bytes;   /* graphs + per-slot reserved scratch */
+} apspie_server_stats;
+
+/* device: GPU ordinal; memory_budget_bytes: device bytes the server may hold (graphs,
+ * scratch, batch staging); num_slots: concurrent launches (1..16); max_batch: BFS
+ * requests per launch. */
+apspie_status apspie_server_create(int device, int64_t memory_budget_bytes, int32_t num_slots,
+                                   int32_t max_batch, apspie_server **out);
+/* Uploads a graph (host CSR; int32 weights enable SSSP). symmetric != 0 marks it
+ * undirected. MIS priorities are mt19937(mis_seed) outputs per vertex. Before start only. */
+apspie_status apspie_server_add_graph(apspie_server *s, const apspie_host_csr *g, int32_t symmetric,
+                                      uint32_t mis_seed, int32_t *graph_id);
+/* Reserves the slots' scratch and starts the worker thread. */
+apspie_status apspie_server_start(apspie_server *s);
+/* Queues a request; the answer is written to d_out (device memory of the server's GPU),
+ * which must stay valid until the request completes. Thread-safe. */
+apspie_status apspie_server_submit(apspie_server *s, int32_t graph_id, int32_t kind, int32_t source,
+                                   void *d_out, uint64_t *ticket);
+/* Blocks until the request completes (timeout_ms < 0: no limit); returns its status and
+ * the latency from submit to completion in *latency_ms. A ticket can be waited once. */
+apspie_status apspie_server_wait(apspie_server *s, uint64_t ticket, int32_t timeout_ms,
+                                 double *latency_ms);
+/* Non-blocking completion test. */
+apspie_status apspie_server_poll(apspie_server *s, uint64_t ticket, int32_t *done);
+apspie_status apspie_server_get_stats(apspie_server *s, apspie_server_stats *out);
+/* Drains outstanding requests, stops the worker and frees the server. */
+void apspie_server_destroy(apspie_server *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APSPIE_SERVER_H */

@@ -1,0 +1,118 @@
+"""GPU tests of the query server: answers identical to the plain path alone and in a mix,
+continuous batching actually folds requests, and the memory budget is enforced."""
+import numpy as np
+import pytest
+
+import apspie_b200 as ap
+from apspie_b200 import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def graphs():
+    return [ap.gen_rmat(s, 16, 20 + s, 3) for s in (10, 12, 14)]
+
+
+def _plain(ctx, g, kind, src):
+    import torch
+
+    dg = ap.DeviceGraph(g)
+    if kind == L.QUERY_BFS:
+        return ctx.bfs(dg, src).cpu().numpy()
+    if kind == L.QUERY_SSSP:
+        return ctx.sssp(dg, src).cpu().numpy()
+    pr = torch.from_numpy(ap.mt19937_u32(4, g.m).view(np.int32)).cuda()
+    return ctx.mis(dg, pr).cpu().numpy()
+
+
+def _out(g, kind):
+    import torch
+
+    return torch.empty(g.m, dtype=torch.uint8 if kind == L.QUERY_MIS else torch.int32, device="cuda")
+
+
+def test_server_mix_matches_plain_path_alone_and_in_mix(ctx, graphs):
+    srv = ap.Server(0, budget_bytes=8 << 30, slots=2, max_batch=512)
+    gids = [srv.add_graph(g) for g in graphs]
+    srv.start()
+    rng = np.random.default_rng(7)
+    kinds = rng.choice([L.QUERY_BFS, L.QUERY_SSSP, L.QUERY_MIS], size=400, p=[0.7, 0.25, 0.05])
+    which = rng.integers(0, len(graphs), 400)
+    srcs = [int(rng.integers(0, graphs[w].m)) for w in which]
+    # one request alone
+    k0, w0, s0 = int(kinds[0]), int(which[0]), srcs[0]
+    alone = _out(graphs[w0], k0)
+    srv.wait(srv.submit(gids[w0], k0, s0, alone))
+    # all of them in a burst (the first one again, now in the mix)
+    outs, tickets = [], []
+    for k, w, s in zip(kinds, which, srcs):
+        o = _out(graphs[w], int(k))
+        outs.append(o)
+        tickets.append(srv.submit(gids[w], int(k), s, o))
+    lat = [srv.wait(t) for t in tickets]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == 401 and st["failed"] == 0
+    assert st["launches"] < st["completed"]  # requests were folded into shared launches
+    assert st["max_batch_seen"] > 1
+    cache = {}
+    for k, w, s, o in zip(kinds, which, srcs, outs):
+        key = (int(k), int(w), s if k != L.QUERY_MIS else -1)
+        if key not in cache:
+            cache[key] = _plain(ctx, graphs[w], int(k), s)
+        np.testing.assert_array_equal(o.cpu().numpy(), cache[key], err_msg=str(key))
+    np.testing.assert_array_equal(alone.cpu().numpy(), outs[0].cpu().numpy())
+    assert min(lat) > 0
+
+
+def test_server_budget_enforced(graphs):
+    g = graphs[2]
+    need = (g.m + 1) * 4 + g.nnz * 8 + g.m * 4
+    with pytest.raises(ap.ApspieError):
+        srv = ap.Server(0, budget_bytes=need // 2, slots=1)
+        try:
+            srv.add_graph(g)
+        finally:
+            srv.close()
+
+
+def test_server_tight_budget_shrinks_batches_but_answers_stay_exact(ctx, graphs):
+    g = graphs[2]
+    probe = ap.Server(0, budget_bytes=4 << 30, slots=1)
+    probe.add_graph(g)
+    probe.start()
+    resident = probe.stats()["resident_bytes"]
+    probe.close()
+    # room for the graph, the slot's scratch and about ten BFS output rows at a time
+    budget = resident + 10 * g.m * 4 + 4096
+    srv = ap.Server(0, budget_bytes=budget, slots=1, max_batch=512)
+    gid = srv.add_graph(g)
+    srv.start()
+    srcs = ap.lcc_sample(g, 64, 5)
+    outs = [_out(g, L.QUERY_BFS) for _ in srcs]
+    ts = [srv.submit(gid, L.QUERY_BFS, int(s), o) for s, o in zip(srcs, outs)]
+    for t in ts:
+        srv.wait(t)
+    st = srv.stats()
+    srv.close()
+    assert st["peak_bytes"] <= budget
+    assert st["max_batch_seen"] < 64
+    for s, o in zip(srcs, outs):
+        np.testing.assert_array_equal(o.cpu().numpy(), _plain(ctx, g, L.QUERY_BFS, int(s)))
+
+
+def test_server_rejects_bad_requests(graphs):
+    import torch
+
+    srv = ap.Server(0, budget_bytes=2 << 30, slots=1)
+    gid = srv.add_graph(ap.HostGraph(graphs[0].m, graphs[0].n, graphs[0].row_ptr, graphs[0].col_ind, None, True))
+    srv.start()
+    o = torch.empty(graphs[0].m, dtype=torch.int32, device="cuda")
+    with pytest.raises(ap.ApspieError):
+        srv.submit(gid, L.QUERY_BFS, graphs[0].m, o)  # source out of range
+    with pytest.raises(ap.ApspieError):
+        srv.submit(gid, L.QUERY_SSSP, 0, o)  # no weights on this graph
+    with pytest.raises(ap.ApspieError):
+        srv.submit(gid + 1, L.QUERY_BFS, 0, o)
+    srv.close()
