@@ -108,6 +108,7 @@ SIGNATURES = {
     "apspie_spmspv_bool": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p]),
     "apspie_bfs_batch": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_int32, c_int32, c_void_p,
                                  POINTER(RunStats)]),
+    "apspie_sssp_batch": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_int32, c_void_p, POINTER(RunStats)]),
     "apspie_bfs_noalloc": (c_int, [POINTER(CSR), c_int32, c_int32, c_void_p, c_void_p, POINTER(RunStats)]),
     # SpGEMM / TC
     "apspie_spgemm": (c_int, [c_void_p, POINTER(CSR), POINTER(CSR), POINTER(CSROwned)]),

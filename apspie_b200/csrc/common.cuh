@@ -95,6 +95,7 @@ apspie_status finish_call(apspie_ctx *ctx, apspie_run_stats *stats, const char *
 size_t traversal_scratch_need(int m);        // apspie_bfs / apspie_sssp
 size_t mis_scratch_need(int m);              // apspie_mis
 size_t bfs_batch_scratch_need(int m, int nq);  // apspie_bfs_batch (nq <= 512 per launch)
+size_t sssp_batch_scratch_need(int m, int nq);  // apspie_sssp_batch (nq <= 512 per launch)
 
 // Device-wide exclusive scan (scan.cu): out[0..n) = prefix of in, out[n] = total.
 size_t scan_scratch_bytes(long long n);

@@ -47,13 +47,18 @@ struct ExpandSmem {
     Warp w[NWARP];
 };
 
+struct RowIsEntry {
+    __device__ __forceinline__ int operator()(int e) const { return e; }
+};
+
 // Phase A over this block's chunk of queue q[0, nf). hook(i, v, deg) may rewrite the
-// degree (e.g. 0 for an entry that needs no expansion) and do per-entry work.
-template <int BLOCK, class Hook>
+// degree (e.g. 0 for an entry that needs no expansion) and do per-entry work; the CSR row
+// of queue entry e is row_of(e) (the entry itself unless the entry packs more).
+template <int BLOCK, class Hook, class RowOf = RowIsEntry>
 __device__ __forceinline__ void frontier_phase_a(const int *__restrict__ q, int nf,
                                                  const int *__restrict__ row_ptr, int *rs,
                                                  int *loc_off, int *chunk_sum, int *scan_tmp,
-                                                 Hook hook) {
+                                                 Hook hook, RowOf row_of = RowOf()) {
     const int G = gridDim.x;
     const int C = (nf + G - 1) / G;
     const int c0 = min(static_cast<int>(blockIdx.x) * C, nf);
@@ -64,8 +69,9 @@ __device__ __forceinline__ void frontier_phase_a(const int *__restrict__ q, int 
         int deg = 0;
         if (i < c1) {
             const int v = __ldcg(q + i);
-            const int r0 = __ldg(row_ptr + v);
-            deg = __ldg(row_ptr + v + 1) - r0;
+            const int row = row_of(v);
+            const int r0 = __ldg(row_ptr + row);
+            deg = __ldg(row_ptr + row + 1) - r0;
             deg = hook(i, v, deg);
             rs[i] = r0;
         }

@@ -11,7 +11,7 @@
 //           into each request's output buffer;
 //   MIS  -> one apspie_mis (the fixed priorities make every MIS query on a graph the same
 //           question), the set copied to every waiting request;
-//   SSSP -> apspie_sssp per request, back to back on the slot's stream.
+//   SSSP -> apspie_sssp_batch over up to max_batch sources, rows copied likewise.
 // A launch is admitted only if resident graphs + the slots' reserved scratch + the batch's
 // output staging fit the budget; otherwise it waits for a running launch to finish.
 // Requests that arrive while launches run are picked up by the next free slot (no wait for
@@ -101,12 +101,12 @@ namespace {
 // Scratch the launch reserves in the slot's arena, and batch output staging.
 size_t arena_need(const apspie_csr &g, int kind, int n) {
     if (kind == APSPIE_QUERY_BFS) return bfs_batch_scratch_need(g.m, n);
-    if (kind == APSPIE_QUERY_MIS) return mis_scratch_need(g.m);
-    return traversal_scratch_need(g.m);
+    if (kind == APSPIE_QUERY_SSSP) return sssp_batch_scratch_need(g.m, n);
+    return mis_scratch_need(g.m);
 }
 
 size_t stage_need(const apspie_csr &g, int kind, int n) {
-    return kind == APSPIE_QUERY_BFS ? static_cast<size_t>(n) * g.m * 4 : 0;
+    return kind == APSPIE_QUERY_MIS ? 0 : static_cast<size_t>(n) * g.m * 4;
 }
 
 // Device bytes a slot holds now (its arena never shrinks; staging is kept for reuse).
@@ -122,7 +122,7 @@ size_t slot_growth(const Slot &sl, const apspie_csr &g, int kind, int n) {
     const size_t an = arena_need(g, kind, n);
     const size_t sn = stage_need(g, kind, n);
     return (an > cur ? an + an / 8 - cur : 0) + (sn > sl.stage_cap ? sn - sl.stage_cap : 0) +
-           (kind == APSPIE_QUERY_BFS && sl.src_cap < n ? static_cast<size_t>(std::max(n, 512)) * 4 : 0);
+           (kind != APSPIE_QUERY_MIS && sl.src_cap < n ? static_cast<size_t>(std::max(n, 512)) * 4 : 0);
 }
 
 void finish_batch(apspie_server *s, Slot &sl) {
@@ -148,7 +148,7 @@ void launch_batch(apspie_server *s, Slot &sl) {
     const Graph &g = s->graphs[sl.batch.front().graph];
     apspie_status st = APSPIE_OK;
     const int n = static_cast<int>(sl.batch.size());
-    if (sl.kind == APSPIE_QUERY_BFS) {
+    if (sl.kind == APSPIE_QUERY_BFS || sl.kind == APSPIE_QUERY_SSSP) {
         std::vector<int32_t> srcs(n);
         for (int i = 0; i < n; ++i) srcs[i] = sl.batch[i].source;
         const size_t rows = static_cast<size_t>(n) * g.view.m * sizeof(int32_t);
@@ -180,7 +180,9 @@ void launch_batch(apspie_server *s, Slot &sl) {
             cudaMemcpyAsync(sl.d_src, srcs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sl.stream);
             // the host vector must outlive the copy
             cudaStreamSynchronize(sl.stream);
-            st = apspie_bfs_batch(sl.ctx, &g.view, sl.d_src, n, 0, static_cast<int32_t *>(sl.stage), nullptr);
+            st = sl.kind == APSPIE_QUERY_BFS
+                     ? apspie_bfs_batch(sl.ctx, &g.view, sl.d_src, n, 0, static_cast<int32_t *>(sl.stage), nullptr)
+                     : apspie_sssp_batch(sl.ctx, &g.view, sl.d_src, n, static_cast<int32_t *>(sl.stage), nullptr);
         }
         if (st == APSPIE_OK)
             for (int i = 0; i < n; ++i)
@@ -192,9 +194,6 @@ void launch_batch(apspie_server *s, Slot &sl) {
         if (st == APSPIE_OK)
             for (int i = 1; i < n; ++i)
                 cudaMemcpyAsync(sl.batch[i].d_out, first, g.view.m, cudaMemcpyDeviceToDevice, sl.stream);
-    } else {
-        for (int i = 0; i < n && st == APSPIE_OK; ++i)
-            st = apspie_sssp(sl.ctx, &g.view, sl.batch[i].source, static_cast<int32_t *>(sl.batch[i].d_out), nullptr);
     }
     sl.status = st;
     cudaEventRecord(sl.ev, sl.stream);
@@ -234,8 +233,7 @@ void worker_loop(apspie_server *s) {
             const int gi = best->first.first, kind = best->first.second;
             const Graph &g = s->graphs[gi];
             int n = static_cast<int>(best->second.size());
-            if (kind == APSPIE_QUERY_BFS) n = std::min(n, s->max_batch);
-            if (kind == APSPIE_QUERY_SSSP) n = std::min(n, 4);
+            if (kind != APSPIE_QUERY_MIS) n = std::min(n, s->max_batch);
             size_t held = s->graph_bytes;
             for (auto &other : s->slots) held += slot_held(other);
             size_t need = slot_growth(sl, g.view, kind, n);

@@ -289,6 +289,21 @@ class Context:
         self.bfs_batch_into(g, sources, out, depth_cap)
         return out
 
+    def sssp_batch_into(self, g: DeviceGraph, sources, out, stats: bool = False):
+        """sources: int32 CUDA tensor [nq]; out: int32 CUDA tensor [nq, m] (query-major)."""
+        st = L.RunStats() if stats else None
+        self._check(L.lib().apspie_sssp_batch(self.handle, ctypes.byref(g.view(True)), sources.data_ptr(),
+                                              int(sources.shape[0]), out.data_ptr(),
+                                              ctypes.byref(st) if st else None), "sssp_batch")
+        return st.as_dict() if st else None
+
+    def sssp_batch(self, g: DeviceGraph, sources):
+        import torch
+
+        out = torch.empty((int(sources.shape[0]), g.m), dtype=torch.int32, device=f"cuda:{self.device}")
+        self.sssp_batch_into(g, sources, out)
+        return out
+
     # ---- SpGEMM / TC
     def spgemm(self, A: DeviceGraph, B: DeviceGraph):
         """C = A*B -> (row_ptr, col_ind, val) numpy arrays (copied back, library memory freed)."""

@@ -160,6 +160,13 @@ apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, const int32
                                int32_t num_sources, int32_t depth_cap, int32_t *d_depths,
                                apspie_run_stats *stats);
 
+/* Batched multi-source SSSP over int32 weights: num_sources queries in one persistent
+ * launch per group (a group holds 32*W queries with (nnz + m) * W < 2^31, W <= 16).
+ * d_dists is num_sources x m int32, query-major (row q = what apspie_sssp returns for
+ * d_sources[q]); -1 unreached. */
+apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources,
+                                int32_t num_sources, int32_t *d_dists, apspie_run_stats *stats);
+
 /* BFS that allocates nothing, for callers that cannot call cudaMalloc: code running where
  * device allocation is forbidden or unavailable (inside another allocator's memory budget,
  * a host that reserves all device memory up front, a plugin loaded into such a process).

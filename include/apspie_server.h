@@ -4,8 +4,8 @@
  * No reference counterpart: the reference answers one query per process run
  * (test/bfs/run.sh, test/sssp/run.sh, test/mis/run.sh). The server keeps several graphs on
  * one GPU, admits BFS / SSSP / MIS requests against a device-memory budget and folds
- * requests that wait on the same graph into one launch (BFS: apspie_bfs_batch; MIS: one
- * apspie_mis shared by all waiting requests; SSSP: apspie_sssp per request), on several
+ * requests that wait on the same graph into one launch (BFS: apspie_bfs_batch; SSSP:
+ * apspie_sssp_batch; MIS: one apspie_mis shared by all waiting requests), on several
  * execution slots whose launches overlap on the device. Each answer is written by the same
  * kernels as the plain entry points, so it is identical alone or in a mix.
  */

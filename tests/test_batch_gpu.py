@@ -93,3 +93,38 @@ def test_batch_rmat22_full_size(ctx):
     out = ctx.bfs_batch(dg, s)
     for q in (0, 63, 127):
         np.testing.assert_array_equal(out[q].cpu().numpy(), oracle.bfs(g.row_ptr, g.col_ind, int(s[q])))
+
+
+# ------------------------------------------------------------------ batched SSSP
+@pytest.mark.parametrize("nq", [1, 7, 32, 100, 512])
+def test_sssp_batch_rows_equal_single_sssp(ctx, rmat14, nq):
+    g, dg = rmat14
+    s = _srcs(g, nq, 4)
+    out = ctx.sssp_batch(dg, s).cpu().numpy()
+    for q in sorted({0, nq // 2, nq - 1}):
+        np.testing.assert_array_equal(out[q], oracle.sssp(g.row_ptr, g.col_ind, g.val, int(s[q])), err_msg=f"q{q}")
+    for q in range(0, nq, max(1, nq // 8)):
+        np.testing.assert_array_equal(out[q], ctx.sssp(dg, int(s[q])).cpu().numpy())
+
+
+def test_sssp_batch_duplicates_and_unreached(ctx, golden):
+    import torch
+
+    rp, ci = golden["test_cc_u_row_ptr"], golden["test_cc_u_col_ind"]
+    w = golden["test_cc_u_w"]
+    g = ap.HostGraph(rp.shape[0] - 1, rp.shape[0] - 1, rp, ci, w, True)
+    srcs = torch.tensor([0, 3, 3, 9, 0], dtype=torch.int32, device="cuda")
+    out = ctx.sssp_batch(ap.DeviceGraph(g), srcs).cpu().numpy()
+    for q, s in enumerate(srcs.cpu().numpy().tolist()):
+        np.testing.assert_array_equal(out[q], golden["test_cc_u_sssp"][s])
+
+
+def test_sssp_batch_rmat20_full_size(ctx):
+    import torch
+
+    g = ap.gen_rmat(20, 16, 2, 3)
+    dg = ap.DeviceGraph(g)
+    s = torch.from_numpy(ap.lcc_sample(g, 64, 6)).cuda()
+    out = ctx.sssp_batch(dg, s)
+    for q in (0, 63):
+        np.testing.assert_array_equal(out[q].cpu().numpy(), oracle.sssp(g.row_ptr, g.col_ind, g.val, int(s[q])))
