@@ -94,6 +94,7 @@ SIGNATURES = {
     "apspie_ctx_set_validate": (c_int, [c_void_p, c_int]),
     "apspie_ctx_set_bfs_tuning": (c_int, [c_void_p, c_float, c_float]),
     "apspie_ctx_set_sssp_delta": (c_int, [c_void_p, c_int32]),
+    "apspie_ctx_set_sssp_band": (c_int, [c_void_p, c_int64]),
     "apspie_ctx_set_max_grid": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_set_batch_push_frac": (c_int, [c_void_p, c_float]),
     "apspie_ctx_scratch_bytes": (c_int64, [c_void_p]),

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include <string>
@@ -13,13 +14,15 @@
 namespace apspie {
 
 constexpr int kTimeline = 128;
+constexpr int kBandBins = 256;  // SSSP distance-band histogram bins
 
 // ---------------------------------------------------------------------------------
 // Per-call device control block. Reset by the host (one memset) before each launch.
 // ---------------------------------------------------------------------------------
 struct TravCtl {
-    unsigned bar_count;  // grid barrier arrival counter
-    unsigned bar_gen;    // grid barrier generation
+    // grid barrier word: arrivals count in the low bits, the phase flips bit 31. It sits
+    // next to `err` in one aligned 8-byte pair so a single load returns both.
+    unsigned bar;
     int err;             // first apspie_status error raised on the device
     int err_where;       // kernel-defined location code of that error
     int qlen[2];         // frontier queue lengths (ping-pong)
@@ -35,10 +38,17 @@ struct TravCtl {
     int tl_count;        // phase timeline: block 0 stamps every grid barrier it passes
     int tl_site[kTimeline];
     unsigned long long tl_ns[kTimeline];
+    // SSSP distance band (ping-pong with the frontier queues): the least distance in each
+    // queue and a degree-weighted histogram of its distances. Device-only.
+    int sbase[2];
+    unsigned long long shist[2][kBandBins];
 };
+static_assert(offsetof(TravCtl, bar) == 0 && offsetof(TravCtl, err) == 4, "barrier word / error pair");
+// Prefix of the control block the host reads back after a call.
+constexpr size_t kCtlHostBytes = offsetof(TravCtl, sbase);
 
 // Upper bound on a persistent grid (chunk sums are staged in shared memory).
-constexpr int kMaxGrid = 2048;
+constexpr int kMaxGrid = 1024;
 // A grid barrier gives up after this long (ns) and raises APSPIE_ERR_TIMEOUT.
 constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;
 
@@ -64,6 +74,7 @@ struct apspie_ctx {
     float bfs_alpha = 14.0f;
     float bfs_beta = 24.0f;
     int sssp_delta = 0;  // <= 0: chosen on the device
+    long long sssp_band = 0;  // 0: auto, < 0: off
     int max_grid = 0;    // 0: as many co-resident blocks as fit
     float batch_push_frac = 0.05f;  // batched BFS: push while frontier edges < frac * nnz
 };
@@ -163,38 +174,46 @@ __device__ __forceinline__ void raise_error(TravCtl *ctl, int *sticky, int statu
     atomicCAS(sticky, 0, status);
 }
 
-// Grid-wide barrier for a cooperatively launched (co-resident) grid. Every wait is
-// bounded by kBarrierTimeoutNs; on timeout it raises APSPIE_ERR_TIMEOUT and returns
-// false, as it does whenever any block has raised an error, so that all blocks leave
-// the persistent loop together instead of hanging.
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const void *p) {
+    unsigned long long v;
+    asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier for a cooperatively launched (co-resident) grid: a sense-reversing
+// counter. Thread 0 of every block adds 1 to ctl->bar, except block 0, which adds
+// 2^31 - (G - 1); the G additions sum to 2^31, so bit 31 flips exactly when the last block
+// arrives and the low bits return to where they were (no reset). A waiter polls the pair
+// (bar, err) with one 64-bit load until bit 31 differs from what it saw before arriving,
+// or until an error is posted. Every wait is bounded by kBarrierTimeoutNs; on timeout it
+// raises APSPIE_ERR_TIMEOUT. Returns false when any block has raised an error, so that all
+// blocks leave the persistent loop together instead of hanging.
 __device__ __forceinline__ bool grid_barrier(TravCtl *ctl, int *sticky, int where) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned nblocks = gridDim.x;
-        unsigned gen = ld_acquire_u32(&ctl->bar_gen);
+        const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
         __threadfence();
-        unsigned prev = atomicAdd(&ctl->bar_count, 1u);
-        if (prev == nblocks - 1) {
-            ctl->bar_count = 0;
-            __threadfence();
-            st_release_u32(&ctl->bar_gen, gen + 1);
-        } else {
-            unsigned long long t0 = globaltimer_ns();
-            while (ld_acquire_u32(&ctl->bar_gen) == gen) {
-                if (ld_volatile_i32(&ctl->err) != 0) { ok = 0; break; }
-                __nanosleep(100);
-                if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+        const unsigned before = atomicAdd(&ctl->bar, inc);
+        unsigned long long pair;
+        unsigned long long t0 = 0;
+        for (unsigned spin = 1;; ++spin) {
+            pair = ld_volatile_u64(&ctl->bar);
+            if (((static_cast<unsigned>(pair) ^ before) & 0x80000000u) != 0u) break;
+            if ((pair >> 32) != 0ull) break;  // an error was raised: leave now
+            if ((spin & 1023u) == 0u) {
+                const unsigned long long t = globaltimer_ns();
+                if (t0 == 0) {
+                    t0 = t;
+                } else if (t - t0 > kBarrierTimeoutNs) {
                     raise_error(ctl, sticky, APSPIE_ERR_TIMEOUT, where);
-                    ok = 0;
+                    pair = 1ull << 32;
                     break;
                 }
             }
         }
         __threadfence();
-        if (ld_volatile_i32(&ctl->err) != 0) ok = 0;
-        s_ok = ok;
+        s_ok = (pair >> 32) == 0ull;
         timeline_mark(ctl, where);
     }
     __syncthreads();
@@ -231,6 +250,37 @@ __device__ __forceinline__ int block_exclusive_scan(int x, int &total, int *tmp)
     total = tmp[32];
     __syncthreads();
     return res;
+}
+
+// Block-wide inclusive scan of one 64-bit count per thread; `tmp` must hold 33 values and
+// tmp[32] holds the block total on return.
+template <int BLOCK>
+__device__ __forceinline__ unsigned long long block_inclusive_scan_u64(unsigned long long x,
+                                                                      unsigned long long *tmp) {
+    static_assert(BLOCK % 32 == 0 && BLOCK <= 1024, "block size");
+    constexpr int NW = BLOCK / 32;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) tmp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        const unsigned long long w = lane < NW ? tmp[lane] : 0ull;
+        unsigned long long wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        if (lane < NW) tmp[lane] = wi - w;
+        if (lane == NW - 1) tmp[32] = wi;
+    }
+    __syncthreads();
+    return tmp[wid] + incl;
 }
 
 // Warp-aggregated append of `v` to queue `q` for lanes with pred set. All 32 lanes of

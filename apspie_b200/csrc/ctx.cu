@@ -151,7 +151,7 @@ apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, vo
 
 apspie_status finish_call(apspie_ctx *ctx, apspie_run_stats *stats, const char *who) {
     if (!stats) return APSPIE_OK;
-    cudaError_t e = cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(TravCtl),
+    cudaError_t e = cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, kCtlHostBytes,
                                     cudaMemcpyDeviceToHost, ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "stats copy");
     e = cudaStreamSynchronize(ctx->stream);
@@ -263,6 +263,12 @@ apspie_status apspie_ctx_set_bfs_tuning(apspie_ctx *ctx, float alpha, float beta
 apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta) {
     if (!ctx) return APSPIE_ERR_INVALID_ARG;
     ctx->sssp_delta = delta;
+    return APSPIE_OK;
+}
+
+apspie_status apspie_ctx_set_sssp_band(apspie_ctx *ctx, int64_t edges) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    ctx->sssp_band = edges;
     return APSPIE_OK;
 }
 

@@ -26,19 +26,31 @@
 
 namespace apspie {
 
-template <int BLOCK, int VT>
+// Per-warp staging slice. EXTRA adds the second payload and the per-entry accumulator
+// (MIS, batched SSSP); BFS and SSSP leave them out to keep shared memory (occupancy) down.
+template <int WT, bool EXTRA>
+struct WarpSlice {
+    int off[WT + 1];   // global edge offset of each staged entry
+    int rs[WT + 1];    // CSR row start of each staged entry
+    int aux[WT + 1];   // per-entry payload (distance snapshot, vertex id, ...)
+    int aux2[WT + 1];  // second payload (priority, ...)
+    int flag[WT + 1];  // per-entry accumulator flushed after the tile
+    int seg[WT];       // tile edge slot -> staged entry
+};
+template <int WT>
+struct WarpSlice<WT, false> {
+    int off[WT + 1];
+    int rs[WT + 1];
+    int aux[WT + 1];
+    int seg[WT];
+};
+
+template <int BLOCK, int VT, bool EXTRA = true>
 struct ExpandSmem {
     static constexpr int NWARP = BLOCK / 32;
     static constexpr int WT = 32 * VT;  // items (entries + edges) per warp tile
     static constexpr int BATCH = BLOCK; // warp tiles whose splits are found together
-    struct Warp {
-        int off[WT + 1];   // global edge offset of each staged entry
-        int rs[WT + 1];    // CSR row start of each staged entry
-        int aux[WT + 1];   // per-entry payload (distance snapshot, vertex id, ...)
-        int aux2[WT + 1];  // second payload (priority, ...)
-        int flag[WT + 1];  // per-entry accumulator flushed after the tile
-        int seg[WT];       // tile edge slot -> staged entry
-    };
+    using Warp = WarpSlice<WT, EXTRA>;
     static constexpr int QCAP = 128;  // per-warp queue staging (see WarpQueue)
     int qbuf[NWARP][2][QCAP];
     int base[kMaxGrid + 1];  // exclusive prefix of chunk totals
@@ -144,12 +156,12 @@ __device__ __forceinline__ int frontier_merge_path(long long diag, int nf, int E
 // op(valid, k, idx, ws) handles a lane's VT edges (CSR positions idx[], owning staged
 // entries k[]); post(ne, ws) runs after the tile's edges (per-entry flushes). All three
 // are called by every lane of the warp, so they may use warp collectives.
-template <int BLOCK, int VT, class Load, class Op, class Post>
+template <int BLOCK, int VT, bool EXTRA, class Load, class Op, class Post>
 __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__restrict__ loc_off,
                                                 const int *__restrict__ rs,
-                                                ExpandSmem<BLOCK, VT> &sm, Load load, Op op,
+                                                ExpandSmem<BLOCK, VT, EXTRA> &sm, Load load, Op op,
                                                 Post post) {
-    using S = ExpandSmem<BLOCK, VT>;
+    using S = ExpandSmem<BLOCK, VT, EXTRA>;
     constexpr int WT = S::WT;
     constexpr int NWARP = S::NWARP;
     constexpr int BATCH = S::BATCH;

@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
             const int *qc = a.q[cur];
             unsigned *vis = a.vis;
             unsigned *touched = a.touched;
-            frontier_expand<kMsBlock, kMsVT>(
+            frontier_expand<kMsBlock, kMsVT, true>(
                 nA, E, a.loc_off, a.rs, sm, [&](int j, int k, MsWarp &ws) { ws.aux[k] = __ldcg(qc + j); },
                 [&](const bool (&valid)[kMsVT], const int (&kk)[kMsVT], const int (&idx)[kMsVT], MsWarp &ws) {
                     int v[kMsVT];

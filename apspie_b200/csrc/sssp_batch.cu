@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kSbBlock) sssp_batch_kernel(SbArgs a) {
         unsigned *dist = a.dist;
         TravCtl *ctl = a.ctl;
         int *sticky = a.sticky;
-        frontier_expand<kSbBlock, kSbVT>(
+        frontier_expand<kSbBlock, kSbVT, true>(
             nf, E, a.loc_off, a.rs, sm,
             [&](int j, int k, SbWarp &ws) {
                 const int e = __ldcg(qc + j);

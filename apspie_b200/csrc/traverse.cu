@@ -17,14 +17,33 @@ namespace apspie {
 
 namespace {
 
+// Build-time knobs of the SSSP kernel (defaults are the tuned values).
+#ifndef APSPIE_SSSP_VT
+#define APSPIE_SSSP_VT 4
+#endif
+#ifndef APSPIE_SSSP_MINB
+#define APSPIE_SSSP_MINB 4
+#endif
+#ifndef APSPIE_SSSP_PREREAD
+#define APSPIE_SSSP_PREREAD 1
+#endif
+
+
 constexpr int kBlock = 256;
 constexpr int kVT = 4;
-using Smem = ExpandSmem<kBlock, kVT>;
+using Smem = ExpandSmem<kBlock, kVT>;          // MIS (uses the extra per-entry arrays)
 using WarpSlice = Smem::Warp;
+using BfsSmem = ExpandSmem<kBlock, kVT, false>;
+using BfsSlice = BfsSmem::Warp;
+constexpr int kSsspVT = APSPIE_SSSP_VT;
+constexpr int kSsspPA = 4;  // frontier entries per thread per phase-A step
+using SsspSmem = ExpandSmem<kBlock, kSsspVT, false>;
+using SsspSlice = SsspSmem::Warp;
 using WQ = WarpQueue<Smem::QCAP>;
 
 struct NoPost {
-    __device__ void operator()(int, WarpSlice &) const {}
+    template <class S>
+    __device__ void operator()(int, S &) const {}
 };
 
 constexpr int kInf = 0x7fffffff;
@@ -102,7 +121,7 @@ struct BfsArgs {
 // edges still unexplored (m_u): push->pull when m_f > m_u/alpha, pull->push when the
 // frontier holds fewer than m/beta vertices. Depth results do not depend on the choice.
 __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
-    __shared__ Smem sm;
+    __shared__ BfsSmem sm;
     timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
     const int gtid = blockIdx.x * kBlock + threadIdx.x;
@@ -168,10 +187,10 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
             ++npush;
             const int *col = a.col_ind;
             int *depth = a.depth;
-            frontier_expand<kBlock, kVT>(
-                nf, E, a.buf.loc_off, a.buf.rs, sm, [](int, int, WarpSlice &) {},
+            frontier_expand<kBlock, kVT, false>(
+                nf, E, a.buf.loc_off, a.buf.rs, sm, [](int, int, BfsSlice &) {},
                 [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT],
-                    WarpSlice &) {
+                    BfsSlice &) {
                     int v[kVT];
                     unsigned word[kVT];
 #pragma unroll
@@ -242,6 +261,7 @@ struct SsspArgs {
     int m, nnz, src, delta_hint;
     int is_float;        // weights/distances are non-negative float32 held as their bit patterns
     int unreached_bits;  // written for unreached vertices (int -1, or a float's bits)
+    long long band;      // edges per iteration of the distance band; <= 0: whole frontier
     const int *__restrict__ row_ptr;
     const int *__restrict__ col_ind;
     const int *__restrict__ w;
@@ -254,18 +274,52 @@ struct SsspArgs {
     int *sticky;
 };
 
+// Histogram bin of distance d above the band base hb: 8 linear bins, then 8 bins per
+// octave (three mantissa bits), 256 in all. Integer distances count in units of 1; float
+// distances in units of 1/inv_unit.
+__device__ __forceinline__ int band_bin(int d, int hb, int is_float, float inv_unit) {
+    if (d <= hb) return 0;
+    if (!is_float) {
+        const unsigned x = static_cast<unsigned>(d) - static_cast<unsigned>(hb);
+        if (x < 8u) return static_cast<int>(x);
+        const int e = 31 - __clz(x);
+        return 8 * (e - 2) + static_cast<int>((x >> (e - 3)) & 7u);
+    }
+    const float x = (__int_as_float(d) - __int_as_float(hb)) * inv_unit;
+    if (x < 8.0f) return static_cast<int>(x);
+    const unsigned b = __float_as_uint(x);
+    const int e = static_cast<int>(b >> 23) - 127;
+    const int bin = 8 * (e - 2) + static_cast<int>((b >> 20) & 7u);
+    return bin < kBandBins - 1 ? bin : kBandBins - 1;
+}
+
+struct SsspShared {
+    SsspSmem ex;
+    unsigned long long hist[kBandBins];  // this block's share of the next band histogram
+    unsigned long long scan[33];
+    int hmin;                            // least distance this block queued
+    int dbase;                           // where this block's deferred entries go
+};
+
 // Min-plus SpMSpV iterated to the fixed point with near/far buckets (delta-stepping in
 // the near-far form): the frontier holds the vertices whose distance dropped below the
 // current threshold T; a relaxation that lands at or above T parks the vertex on the far
 // pile instead. When the near frontier empties, T advances by delta and the far pile is
 // split into the new near frontier and what stays far. A vertex is expanded again only
-// if its distance changed since its last expansion. The reference expands every finite
+// if its distance changed since its last expansion. Within the near frontier only the band
+// of lowest distances carrying about a.band edges is expanded per iteration; the rest wait
+// in the queue. The band's cut comes from a degree-weighted histogram of the distances
+// queued during the previous iteration, taken relative to that queue's least distance,
+// which is tracked exactly, and the vertices at that least distance always expand, so
+// every iteration makes progress. The reference expands every finite
 // vertex each iteration (src/spmspvSssp.cuh:31-36, sort + ReduceByKey(min) :220-232) and
 // stops after the CPU BFS depth; here a relaxation is a plain read of dist[v] and, only
 // if it improves, an atomicMin, and the loop ends when both piles are empty. The result is
 // the exact fixed point for non-negative integer weights, independent of relaxation order.
-__global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
-    __shared__ Smem sm;
+__global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs a) {
+    static_assert(kBlock == kBandBins, "one histogram bin per thread");
+    __shared__ SsspShared sh;
+    SsspSmem &sm = sh.ex;
     timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
     const int gtid = blockIdx.x * kBlock + threadIdx.x;
@@ -290,7 +344,7 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
     // sample the weights for the default bucket width
     constexpr int kSample = 1 << 16;
     const int nsamp = a.nnz < kSample ? a.nnz : kSample;
-    if (a.delta_hint <= 0) {
+    {
         double ws = 0.0;
         for (int k = gtid; k < nsamp; k += gstride) {
             const int wb = __ldg(a.w + static_cast<long long>(k) * a.nnz / nsamp);
@@ -305,19 +359,29 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
         a.ctl->qlen[1] = 0;
         a.ctl->flen[0] = 0;
         a.ctl->flen[1] = 0;
+        a.ctl->sbase[0] = 0;  // the source's distance
+        a.ctl->sbase[1] = INF;
     }
+    sh.hist[threadIdx.x] = 0ull;
+    if (threadIdx.x == 0) sh.hmin = INF;
     if (!grid_barrier(a.ctl, a.sticky, kSiteSssp)) return;
 
+    const bool banded = a.band > 0;
+    const double sum_w = __longlong_as_double(__ldcg(&a.ctl->aux[0]));
+    const double mean_w = nsamp ? sum_w / nsamp : 1.0;
+    // float distances are binned in units of mean weight / 256
+    const float inv_unit = (a.is_float && mean_w > 0.0) ? static_cast<float>(256.0 / mean_w) : 1.0f;
     double delta = a.delta_hint;
-    if (delta <= 0) {
-        const double sum = __longlong_as_double(__ldcg(&a.ctl->aux[0]));
-        const double mean_w = nsamp ? sum / nsamp : 1.0;
+    if (delta <= 0 && banded) {
+        delta = 1e300;  // the band orders the work: no far pile
+    } else if (delta <= 0) {
         const double mean_deg = m ? static_cast<double>(a.nnz) / m : 1.0;
         delta = 32.0 * mean_w / (mean_deg > 1.0 ? mean_deg : 1.0);
         if (!a.is_float) delta = floor(delta);
         if (!(delta >= 1.0)) delta = a.is_float ? (delta > 0.0 ? delta : 1.0) : 1.0;
     }
     double thresh = delta;
+    int hb = 0;  // base of the histogram in ctl->shist[cur] (the previous iteration's base)
     int cur = 0, fc = 0;
     long long expanded = 0;
     int iters = 0, steps = 0;
@@ -354,6 +418,7 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                         atomicAnd(infar + (v >> 5), ~(1u << (v & 31)));
                         const unsigned bit = 1u << (v & 31);
                         to_near = !(atomicOr(inq + (v >> 5), bit) & bit);
+                        atomicMin(&a.ctl->sbase[cur], d);
                     } else {
                         stay = true;
                     }
@@ -368,27 +433,122 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
             fc ^= 1;
             continue;
         }
-        int *qlen_next = &a.ctl->qlen[cur ^ 1];
+        int *qlen_next = &a.ctl->qlen[cur ^ 1];  // zero: reset when that queue was last read
         int *snap = a.buf.aux;
 
-        // phase A: dequeue (clear queued bit), snapshot distance, skip unchanged vertices
-        frontier_phase_a<kBlock>(qc, nf, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum,
-                                 sm.scan_tmp, [&](int i, int v, int deg) {
-                                     atomicAnd(inq + (v >> 5), ~(1u << (v & 31)));
-                                     const int d = __ldcg(dist + v);
-                                     snap[i] = d;
-                                     if (__ldcg(last + v) == d) return 0;
-                                     last[v] = d;
-                                     return deg;
-                                 });
-        if (gtid == 0) *qlen_next = 0;
+        // the band: histogram bins up to the first where the running edge count reaches
+        // a.band (kBandBins = every bin: band off, or too little queued work to cut)
+        const int base_i = ld_volatile_i32(&a.ctl->sbase[cur]);
+        int cut = kBandBins;
+        if (banded) {
+            const unsigned long long h = __ldcg(&a.ctl->shist[cur][threadIdx.x]);
+            const unsigned long long incl = block_inclusive_scan_u64<kBlock>(h, sh.scan);
+            const unsigned long long S = static_cast<unsigned long long>(a.band);
+            const bool reach = sh.scan[32] >= S;
+            const int below = __syncthreads_count(incl < S);
+            if (reach && below < kBandBins - 1) cut = below;
+        }
+        const int hb_prev = hb;
+        hb = base_i;
+        const int is_float_a = a.is_float;
+
+        // phase A: dequeue (clear queued bit), snapshot distance, skip unchanged vertices;
+        // vertices above the band stay queued (re-appended to the next queue, bit kept)
+        {
+            // kSsspPA entries per thread per step, their loads issued together; the chunk
+            // layout (chunk c = entries [c*C, (c+1)*C)) is the one frontier_expand reads
+            constexpr int PA = kSsspPA;
+            const int C = (nf + G - 1) / G;
+            const int c0 = min(static_cast<int>(blockIdx.x) * C, nf);
+            const int c1 = min(c0 + C, nf);
+            const int *rpa = a.row_ptr;
+            int carry = 0;
+            for (int base = c0; base < c1; base += kBlock * PA) {
+                const int i0 = base + static_cast<int>(threadIdx.x) * PA;
+                int v[PA], r0[PA], r1[PA], d[PA], lst[PA], out[PA];
+                bool valid[PA], defer[PA];
+#pragma unroll
+                for (int k = 0; k < PA; ++k) {
+                    valid[k] = i0 + k < c1;
+                    v[k] = valid[k] ? __ldcg(qc + i0 + k) : 0;
+                }
+#pragma unroll
+                for (int k = 0; k < PA; ++k) {
+                    r0[k] = valid[k] ? __ldg(rpa + v[k]) : 0;
+                    r1[k] = valid[k] ? __ldg(rpa + v[k] + 1) : 0;
+                    d[k] = valid[k] ? __ldcg(dist + v[k]) : 0;
+                }
+#pragma unroll
+                for (int k = 0; k < PA; ++k) {
+                    defer[k] = valid[k] && cut < kBandBins && d[k] != base_i &&
+                               band_bin(d[k], hb_prev, is_float_a, inv_unit) > cut;
+                    lst[k] = (valid[k] && !defer[k]) ? __ldcg(last + v[k]) : 0;
+                }
+                int sum = 0;
+#pragma unroll
+                for (int k = 0; k < PA; ++k) {
+                    out[k] = 0;
+                    if (valid[k]) {
+                        snap[i0 + k] = d[k];
+                        a.buf.rs[i0 + k] = r0[k];
+                        if (!defer[k]) {
+                            atomicAnd(inq + (v[k] >> 5), ~(1u << (v[k] & 31)));
+                            if (lst[k] != d[k]) {
+                                last[v[k]] = d[k];
+                                out[k] = r1[k] - r0[k];
+                            }
+                        }
+                    }
+                    sum += out[k];
+                }
+                int ndef = 0;
+#pragma unroll
+                for (int k = 0; k < PA; ++k) {
+                    if (defer[k]) {
+                        atomicAdd(&sh.hist[band_bin(d[k], base_i, is_float_a, inv_unit)],
+                                  static_cast<unsigned long long>(r1[k] - r0[k]));
+                        atomicMin(&sh.hmin, d[k]);
+                    }
+                    ndef += defer[k] ? 1 : 0;
+                }
+                // one scan carries both the edge count (high half) and the deferred count
+                // (low half, at most kBlock * PA per step, so it never carries over)
+                const unsigned long long packed =
+                    (static_cast<unsigned long long>(sum) << 32) | static_cast<unsigned>(ndef);
+                const unsigned long long incl = block_inclusive_scan_u64<kBlock>(packed, sh.scan);
+                const unsigned long long excl = incl - packed;
+                const unsigned long long total = sh.scan[32];
+                if (threadIdx.x == 0 && static_cast<unsigned>(total) != 0u)
+                    sh.dbase = atomicAdd(qlen_next, static_cast<int>(static_cast<unsigned>(total)));
+                __syncthreads();
+                int run = carry + static_cast<int>(excl >> 32);
+                int dpos = sh.dbase + static_cast<int>(static_cast<unsigned>(excl));
+#pragma unroll
+                for (int k = 0; k < PA; ++k) {
+                    if (valid[k]) a.buf.loc_off[i0 + k] = run;
+                    run += out[k];
+                    if (defer[k]) qn[dpos++] = v[k];
+                }
+                carry += static_cast<int>(total >> 32);
+                __syncthreads();  // sh.scan and sh.dbase are reused by the next step
+            }
+            if (threadIdx.x == 0) a.buf.chunk_sum[blockIdx.x] = carry;
+        }
         if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarA)) return;
+        // every block has read this queue's length, base and histogram: reset them for the
+        // iteration that fills this queue next
+        if (gtid < kBandBins) a.ctl->shist[cur][gtid] = 0ull;
+        if (gtid == 0) {
+            a.ctl->qlen[cur] = 0;
+            a.ctl->sbase[cur] = INF;
+        }
 
         const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
         expanded += E;
         ++iters;
         const int *col = a.col_ind;
         const int *wt = a.w;
+        const int *rp = a.row_ptr;
         TravCtl *ctl = a.ctl;
         int *sticky = a.sticky;
         int *flen = &a.ctl->flen[fc];
@@ -396,11 +556,12 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
         const int is_float = a.is_float;
         WQ wn(sm.qbuf[threadIdx.x >> 5][0], qn, qlen_next);
         WQ wf(sm.qbuf[threadIdx.x >> 5][1], fcur, flen);
-        frontier_expand<kBlock, kVT>(
+        frontier_expand<kBlock, kSsspVT, false>(
             nf, E, a.buf.loc_off, a.buf.rs, sm,
-            [&](int j, int k, WarpSlice &ws) { ws.aux[k] = __ldcg(snap + j); },
-            [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT],
-                WarpSlice &ws) {
+            [&](int j, int k, SsspSlice &ws) { ws.aux[k] = __ldcg(snap + j); },
+            [&](const bool (&valid)[kSsspVT], const int (&kk)[kSsspVT], const int (&idx)[kSsspVT],
+                SsspSlice &ws) {
+                constexpr int kVT = kSsspVT;
                 int v[kVT], we[kVT], cd[kVT], nd[kVT];
                 bool imp[kVT];
 #pragma unroll
@@ -410,7 +571,7 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                 }
                 // plain (L1-cacheable) reads: a stale, larger value only costs an extra atomic
 #pragma unroll
-                for (int r = 0; r < kVT; ++r) cd[r] = valid[r] ? dist[v[r]] : 0;
+                for (int r = 0; r < kVT; ++r) cd[r] = (valid[r] && APSPIE_SSSP_PREREAD) ? dist[v[r]] : INF;
 #pragma unroll
                 for (int r = 0; r < kVT; ++r) {
                     imp[r] = false;
@@ -453,6 +614,27 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
                             far[r] = !(atomicOr(infar + (v[r] >> 5), bit) & bit);
                     }
                 }
+                if (banded) {
+                    // every improvement below T (queued now or already) enters the next
+                    // band histogram at its new distance (improvements are a few percent of
+                    // the relaxations, so plain shared-memory atomics rarely collide)
+                    bool rec[kVT];
+                    int dg[kVT];
+#pragma unroll
+                    for (int r = 0; r < kVT; ++r) {
+                        rec[r] = imp[r] && nd[r] < old[r] &&
+                                 (is_float ? static_cast<double>(__int_as_float(nd[r]))
+                                           : static_cast<double>(nd[r])) < T;
+                        dg[r] = rec[r] ? __ldg(rp + v[r] + 1) - __ldg(rp + v[r]) : 0;
+                    }
+#pragma unroll
+                    for (int r = 0; r < kVT; ++r) {
+                        if (!rec[r]) continue;
+                        atomicAdd(&sh.hist[band_bin(nd[r], base_i, is_float, inv_unit)],
+                                  static_cast<unsigned long long>(dg[r]));
+                        atomicMin(&sh.hmin, nd[r]);
+                    }
+                }
 #pragma unroll
                 for (int r = 0; r < kVT; ++r) {
                     wn.push(near[r], v[r]);
@@ -462,6 +644,18 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
             NoPost());
         wn.flush();
         wf.flush();
+        if (banded) {
+            __syncthreads();
+            const unsigned long long hv = sh.hist[threadIdx.x];
+            if (hv) {
+                atomicAdd(&a.ctl->shist[cur ^ 1][threadIdx.x], hv);
+                sh.hist[threadIdx.x] = 0ull;
+            }
+            if (threadIdx.x == 0 && sh.hmin != INF) {
+                atomicMin(&a.ctl->sbase[cur ^ 1], sh.hmin);
+                sh.hmin = INF;
+            }
+        }
         if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarB)) return;
         cur ^= 1;
     }
@@ -491,7 +685,7 @@ __global__ void __launch_bounds__(kBlock) sssp_kernel(SsspArgs a) {
         a.ctl->push_iterations = iters;
         a.ctl->pull_iterations = steps - 1 - iters;  // threshold advances
         a.ctl->edges_expanded = expanded;
-        a.ctl->delta = static_cast<int>(delta);  // truncated for float weights
+        a.ctl->delta = delta < 2147483647.0 ? static_cast<int>(delta) : 0;  // 0: no far pile
     }
 }
 
@@ -573,7 +767,7 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         unsigned char *state = a.state;
         int *blocked = a.blocked;
         const int r = round;
-        frontier_expand<kBlock, kVT>(
+        frontier_expand<kBlock, kVT, true>(
             nf, E, a.buf.loc_off, a.buf.rs, sm,
             [&](int j, int k, WarpSlice &ws) {
                 const int v = __ldcg(qc + j);
@@ -840,6 +1034,14 @@ apspie_status sssp_common(apspie_ctx *ctx, const apspie_csr *A, int32_t source, 
     a.w = static_cast<const int *>(A->val);
     a.dist = static_cast<int *>(d_dist);
     a.delta_hint = ctx->sssp_delta;
+    if (ctx->sssp_band > 0) {
+        a.band = ctx->sssp_band;
+    } else if (ctx->sssp_band == 0) {
+        const long long b = A->nnz / 8;
+        a.band = b < (1LL << 18) ? (1LL << 18) : (b > (1LL << 23) ? (1LL << 23) : b);
+    } else {
+        a.band = 0;
+    }
     a.is_float = is_float ? 1 : 0;
     a.unreached_bits = unreached_bits;
     a.buf = carve_trav(base, A->m);
@@ -961,7 +1163,7 @@ apspie_status apspie_bfs_noalloc(const apspie_csr *A, int32_t source, int32_t de
         return APSPIE_ERR_CUDA;
     }
     TravCtl h;
-    if (cudaMemcpyAsync(&h, ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+    if (cudaMemcpyAsync(&h, ctl, kCtlHostBytes, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
         cudaStreamSynchronize(stream) != cudaSuccess)
         return APSPIE_ERR_CUDA;
     if (stats) {

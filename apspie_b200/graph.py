@@ -214,6 +214,10 @@ class Context:
     def set_sssp_delta(self, delta: int) -> None:
         self._check(L.lib().apspie_ctx_set_sssp_delta(self.handle, delta), "set_sssp_delta")
 
+    def set_sssp_band(self, edges: int) -> None:
+        """Edges expanded per SSSP iteration (lowest-distance band); 0 = auto, < 0 = off."""
+        self._check(L.lib().apspie_ctx_set_sssp_band(self.handle, edges), "set_sssp_band")
+
     def set_batch_push_frac(self, frac: float) -> None:
         self._check(L.lib().apspie_ctx_set_batch_push_frac(self.handle, frac), "set_batch_push_frac")
 

@@ -106,9 +106,15 @@ apspie_status apspie_ctx_set_validate(apspie_ctx *ctx, int on);
 /* Direction-switch thresholds for BFS (Beamer's alpha/beta; defaults 14 and 24).
  * alpha <= 0 forces push on every level. */
 apspie_status apspie_ctx_set_bfs_tuning(apspie_ctx *ctx, float alpha, float beta);
-/* SSSP bucket width (delta-stepping "near/far" threshold step). delta <= 0 (default)
- * picks it on the device from a sample of the weights: 32 * mean weight / mean degree. */
+/* SSSP far-pile threshold step (delta-stepping "near/far" buckets). delta <= 0 (default):
+ * no far pile when the distance band is on (below), else 32 * mean weight / mean degree
+ * from a sample of the weights. */
 apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta);
+/* SSSP distance band: each iteration expands only the frontier vertices of lowest
+ * distance whose edges add up to about `edges` (the rest wait in the frontier), chosen
+ * from a degree-weighted distance histogram gathered on the device. edges == 0 (default):
+ * nnz / 8 clamped to [2^18, 2^23]; edges < 0: off (expand the whole frontier). */
+apspie_status apspie_ctx_set_sssp_band(apspie_ctx *ctx, int64_t edges);
 /* Batched BFS direction switch: a level expands top-down while (active vertices x mean
  * degree) < frac * nnz, else bottom-up (default 0.05; bottom-up only on symmetric graphs). */
 apspie_status apspie_ctx_set_batch_push_frac(apspie_ctx *ctx, float frac);
@@ -136,8 +142,8 @@ apspie_status apspie_bfs(apspie_ctx *ctx, const apspie_csr *A, int32_t source,
                          int32_t depth_cap, int32_t *d_depth, apspie_run_stats *stats);
 
 /* Single-source shortest paths by min-plus SpMSpV over int32 edge weights >= 0
- * (A->val_type == APSPIE_VAL_I32), iterated on the device to the fixed point with
- * near/far buckets of width delta (apspie_ctx_set_sssp_delta).
+ * (A->val_type == APSPIE_VAL_I32), iterated on the device to the fixed point, each
+ * iteration expanding the frontier's lowest-distance band (apspie_ctx_set_sssp_band).
  * d_dist[m] (int32): distance, -1 unreached (the CPU check's convention,
  * src/testSssp.cpp:50). Replaces sssp<Value> (src/sssp.cuh:28) and
  * spmspvSssp (src/spmspvSssp.cuh:92). Returns APSPIE_ERR_INVALID_ARG when a path

@@ -274,6 +274,61 @@ def test_sssp_bucket_width_does_not_change_result(ctx, rmat14, delta):
         ctx.set_sssp_delta(0)
 
 
+@pytest.mark.parametrize("band", [-1, 1, 4096, 0, 1 << 40])
+@pytest.mark.parametrize("delta", [0, 64])
+def test_sssp_band_does_not_change_result(ctx, rmat14, band, delta):
+    """The distance band only orders the work: band 1 expands one histogram bin per
+    iteration (deferring almost the whole frontier every time), -1 and 2^40 never defer."""
+    g, dg, src = rmat14
+    ref = oracle.sssp(g.row_ptr, g.col_ind, g.val, src)
+    ctx.set_sssp_band(band)
+    ctx.set_sssp_delta(delta)
+    try:
+        out = ctx.sssp(dg, src)
+        st = ctx.sssp_into(dg, src, out, stats=True)
+        np.testing.assert_array_equal(out.cpu().numpy(), ref)
+        assert st["edges_expanded"] >= st["edges_component"]
+    finally:
+        ctx.set_sssp_band(0)
+        ctx.set_sssp_delta(0)
+
+
+def test_sssp_band_cuts_rework(ctx, rmat14):
+    """With the default band, re-expansion stays near one pass over the component's edges
+    (a whole-frontier Bellman-Ford pass expands several times more)."""
+    g, dg, src = rmat14
+    out = ctx.sssp(dg, src)
+    banded = ctx.sssp_into(dg, src, out, stats=True)
+    ctx.set_sssp_band(-1)
+    ctx.set_sssp_delta(1 << 20)
+    try:
+        whole = ctx.sssp_into(dg, src, out, stats=True)
+    finally:
+        ctx.set_sssp_band(0)
+        ctx.set_sssp_delta(0)
+    assert banded["edges_expanded"] < whole["edges_expanded"]
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference CPU driver not built")
+@pytest.mark.parametrize("band", [1, 0, -1])
+def test_sssp_f32_band_matches_reference_ssspCPU(ctx, rmat14, band):
+    import torch
+
+    g, _, src = rmat14
+    rows = np.repeat(np.arange(g.m), np.diff(g.row_ptr))
+    lo, hi = np.minimum(rows, g.col_ind), np.maximum(rows, g.col_ind)
+    w = (((lo * 7919 + hi * 104729) % 1000) / 9700.0 + 0.0001).astype(np.float32)
+    dg = ap.DeviceGraph(ap.HostGraph(g.m, g.n, g.row_ptr, g.col_ind, w, True))
+    out = torch.empty(g.m, dtype=torch.float32, device="cuda")
+    ctx.set_sssp_band(band)
+    try:
+        ctx.sssp_f32_into(dg, src, out, unreached=-1.0)
+    finally:
+        ctx.set_sssp_band(0)
+    ref, _ = oracle.ref_sssp_f32(g.row_ptr, g.col_ind, w, src)
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
+
+
 @pytest.mark.parametrize("blocks", [1, 3, 148])
 def test_grid_size_does_not_change_results(ctx, rmat14, blocks):
     import torch
