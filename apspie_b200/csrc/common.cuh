@@ -54,6 +54,16 @@ constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;
 
 }  // namespace apspie
 
+// Plan of the last apspie_spgemm_symbolic call, reused by the numeric call on the same
+// operands while no other call has reserved scratch since (scratch_epoch unchanged).
+struct apspie_spgemm_plan_cache {
+    bool valid = false;
+    unsigned long long epoch = 0;
+    apspie_csr a{}, b{};
+    void *dev[8] = {};        // plan buffers inside the scratch arenas
+    long long host[12] = {};  // bin counts and sizes read back at planning
+};
+
 struct apspie_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -62,6 +72,8 @@ struct apspie_ctx {
     // scratch arena: one device allocation, carved per call, grown on demand
     void *scratch = nullptr;
     size_t scratch_bytes = 0;
+    unsigned long long scratch_epoch = 0;  // bumped by every scratch reservation
+    apspie_spgemm_plan_cache sg_cache;
     // secondary arena for variable-size tables (SpGEMM global tier, ...)
     void *scratch2 = nullptr;
     size_t scratch2_bytes = 0;

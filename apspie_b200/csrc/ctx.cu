@@ -24,6 +24,7 @@ apspie_status cuda_error(apspie_ctx *ctx, cudaError_t e, const char *what) {
 }
 
 apspie_status scratch_reserve(apspie_ctx *ctx, size_t bytes, void **out) {
+    ++ctx->scratch_epoch;
     if (bytes <= ctx->scratch_bytes && ctx->scratch) {
         *out = ctx->scratch;
         return APSPIE_OK;
@@ -48,6 +49,7 @@ apspie_status scratch_reserve(apspie_ctx *ctx, size_t bytes, void **out) {
 }
 
 apspie_status scratch2_reserve(apspie_ctx *ctx, size_t bytes, void **out) {
+    ++ctx->scratch_epoch;
     if (bytes <= ctx->scratch2_bytes && ctx->scratch2) {
         *out = ctx->scratch2;
         return APSPIE_OK;

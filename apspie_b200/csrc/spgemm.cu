@@ -7,9 +7,9 @@
 // every table and a COO->CSR rebuild) and its cuSPARSE csrgemm wrappers
 // (src/spgemm.cuh:344-445, src/tc.cuh:62-165). Results: C's structure is the exact
 // union of products; rows are sorted by column; int32 values are exact; FP32 values of a
-// warp-tier row are summed in increasing position of A's row (the oracle's order, so
-// bit-identical); block/global-tier rows accumulate with atomicAdd (order-dependent
-// rounding only).
+// register-tier row (at most 128 products) are summed in increasing position of A's row
+// (the oracle's order, so bit-identical); block/global-tier rows accumulate with
+// atomicAdd (order-dependent rounding only).
 //
 // Pipeline (all on the context stream):
 //  1. rowinfo: per row, ub = sum of deg_B over A's row (products) -> bin; rows appended to
@@ -17,12 +17,14 @@
 //     reads the bin sizes.
 //  2. symbolic: per bin, count distinct columns per row with a hash set -> cnt[]
 //  3. scan cnt -> row_ptr(C); one sync reads nnz(C) (the caller may allocate C here)
-//  4. numeric: per bin, accumulate values in the hash table, then emit the row sorted:
-//     warp tier by a shared-memory bitonic sort, block/global tiers by ranking entries
-//     against a 64K-column bitmap window (prefix popcounts).
-// Bins: 0 no products | 1 ub <= 32: one warp, 64-slot table | 2 ub <= 128: one warp,
-// 256-slot table | 3 ub <= 1024: one block, 2048-slot shared table | 4 larger: one block,
-// global table of >= 2*ub slots (power of two). Tables stay at most half full.
+//  4. numeric: register tiers sort the products and sum each column's run; hash tiers
+//     accumulate values in the table, then emit the row sorted by ranking entries against
+//     a 64K-column bitmap window (prefix popcounts).
+// Bins: 0 no products | 1-3 ub <= 32 / 64 / 128: one warp per row, the row's products
+// held in registers (1, 2 or 4 per lane) and sorted by (column, product index) with a
+// register bitonic network; duplicates are then adjacent and summed in product order |
+// 4 ub <= 1024: one block, 2048-slot shared table | 5 larger: one block, global table of
+// >= 2*ub slots (power of two). Tables stay at most half full.
 #include <algorithm>
 #include <cstring>
 
@@ -32,7 +34,9 @@ namespace apspie {
 namespace {
 
 constexpr int kEmptyKey = -1;
-constexpr int kBins = 5;
+constexpr int kBins = 6;
+constexpr int kBinBlock = 4;   // shared-memory hash table tier
+constexpr int kBinGlobal = 5;  // global-memory hash table tier
 constexpr int kBlockTS = 2048;
 constexpr int kSgBlock = 256;
 constexpr int kWindowBits = 65536;  // columns per bitmap window
@@ -44,13 +48,17 @@ struct SgInfo {
     long long global_slots;
 };
 
-__device__ __forceinline__ int bin_of(long long ub, int degA) {
+// reg_ok: B has at most 2^24 columns, so a register-tier key (column << 7 | product)
+// stays below the padding key 0xffffffff.
+__device__ __forceinline__ int bin_of(long long ub, int degA, bool reg_ok) {
     const long long w = ub > degA ? ub : degA;
     if (ub == 0) return 0;
+    if (!reg_ok && w <= 1024) return kBinBlock;
     if (w <= 32) return 1;
-    if (w <= 128) return 2;
-    if (w <= 1024) return 3;
-    return 4;
+    if (w <= 64) return 2;
+    if (w <= 128) return 3;
+    if (w <= 1024) return kBinBlock;
+    return kBinGlobal;
 }
 
 __device__ __forceinline__ unsigned hash_slot(int col, int log2ts) {
@@ -77,25 +85,31 @@ struct Mat {
 };
 
 // ---------------------------------------------------------------- 1. row info / bins
-__global__ void sg_rowinfo(int m, Mat A, Mat B, long long *ub, int *bin_rows, SgInfo *info,
-                           long long *tbl_off) {
-    const int lane = threadIdx.x & 31;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = warp; i < m; i += nwarps) {
-        const int r0 = A.rp[i], r1 = A.rp[i + 1];
+// 8 lanes per row: ub = sum of deg_B over A's row, and the row's bin.
+__global__ void sg_rowinfo(int m, Mat A, Mat B, bool reg_ok, long long *ub, unsigned char *row_bin,
+                           SgInfo *info, long long *tbl_off) {
+    const int sub = threadIdx.x & 7;
+    const int grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const int ngrp = (gridDim.x * blockDim.x) >> 3;
+    const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    for (int i0 = grp - (grp & 3); i0 < m; i0 += ngrp) {  // the warp's 4 groups move together
+        const int i = i0 + (grp & 3);
         long long s = 0;
-        for (int e = r0 + lane; e < r1; e += 32) {
-            const int k = A.ci[e];
-            s += B.rp[k + 1] - B.rp[k];
+        int r0 = 0, r1 = 0;
+        if (i < m) {
+            r0 = __ldg(A.rp + i);
+            r1 = __ldg(A.rp + i + 1);
+            for (int e = r0 + sub; e < r1; e += 8) {
+                const int k = __ldg(A.ci + e);
+                s += __ldg(B.rp + k + 1) - __ldg(B.rp + k);
+            }
         }
-        for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-        if (lane == 0) {
+        for (int o = 4; o; o >>= 1) s += __shfl_down_sync(gmask, s, o, 8);
+        if (i < m && sub == 0) {
             ub[i] = s;
-            const int b = bin_of(s, r1 - r0);
-            const int pos = atomicAdd(&info->bin_count[b], 1);
-            bin_rows[static_cast<long long>(b) * m + pos] = i;
-            if (b == 4) {
+            const int b = bin_of(s, r1 - r0, reg_ok);
+            row_bin[i] = static_cast<unsigned char>(b);
+            if (b == kBinGlobal) {
                 long long ts = 64;
                 while (ts < 2 * s) ts <<= 1;
                 tbl_off[i] = static_cast<long long>(
@@ -106,28 +120,59 @@ __global__ void sg_rowinfo(int m, Mat A, Mat B, long long *ub, int *bin_rows, Sg
     }
 }
 
-// ---------------------------------------------------------------- warp tier
-template <int PL, int TS, typename V>
-struct WarpTierSmem {
-    static constexpr int UB = 32 * PL;
-    int keys[TS];
-    V vals[TS];
-    int sk_rs[UB];    // B row start of each A entry
-    int soff[UB + 1]; // exclusive product offset of each A entry
-    V sa[UB];         // A values
-    int lk[UB];       // extraction list (sorted)
-    V lv[UB];
+// Per-bin row lists (stride m): each block counts its rows per bin with warp ballots,
+// reserves room with one global atomic per bin, then scatters.
+__global__ void sg_binlists(int m, const unsigned char *__restrict__ row_bin, int *bin_rows, SgInfo *info) {
+    __shared__ int cnt[kBins];
+    __shared__ int base[kBins];
+    const int lane = threadIdx.x & 31;
+    for (int c0 = blockIdx.x * blockDim.x; c0 < m; c0 += gridDim.x * blockDim.x) {
+        if (threadIdx.x < kBins) cnt[threadIdx.x] = 0;
+        __syncthreads();
+        const int i = c0 + threadIdx.x;
+        const int b = i < m ? row_bin[i] : -1;
+        int pos = 0;
+#pragma unroll
+        for (int k = 0; k < kBins; ++k) {
+            const unsigned mk = __ballot_sync(0xffffffffu, b == k);
+            int wbase = 0;
+            if (mk && lane == __ffs(mk) - 1) wbase = atomicAdd(&cnt[k], __popc(mk));
+            wbase = __shfl_sync(0xffffffffu, wbase, mk ? __ffs(mk) - 1 : 0);
+            if (b == k) pos = wbase + __popc(mk & ((1u << lane) - 1u));
+        }
+        __syncthreads();
+        if (threadIdx.x < kBins && cnt[threadIdx.x])
+            base[threadIdx.x] = atomicAdd(&info->bin_count[threadIdx.x], cnt[threadIdx.x]);
+        __syncthreads();
+        if (b >= 0) bin_rows[static_cast<long long>(b) * m + base[b] + pos] = i;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- register (warp) tier
+template <int PL, typename V>
+struct RegTierSmem {
+    static constexpr int N = 32 * PL;
+    int soff[N + 1];  // exclusive product offset of each A entry
+    int bs[N];        // B row start of each A entry
+    V av[N];          // A values
+    V pv[N];          // product values, by product index
+    unsigned skey[N]; // sorted keys (numeric: walked by the head of each run)
 };
 
-// One warp per row. Products of A entry t are inserted only after every product of
-// entries < t (the columns of one entry are distinct), so each output value is summed in
-// increasing t exactly as the oracle does.
-template <int PL, int TS, int LOG2TS, bool NUMERIC, typename V>
-__global__ void __launch_bounds__(kSgBlock) sg_warp(const int *__restrict__ rows, int nrows, Mat A, Mat B,
-                                                    int *cnt, const int *__restrict__ crp, int *cci,
-                                                    V *cval, SgInfo *info) {
-    using S = WarpTierSmem<PL, TS, V>;
-    constexpr int UB = S::UB;
+// One warp per row of at most N = 32 * PL products. Product q (element r * 32 + lane) of
+// A entry t gets the key (column << QB) | q; after a bitonic sort of the keys in registers
+// the products of one output column are adjacent and in increasing q, i.e. increasing
+// position in A's row, so a run's head sums them in the oracle's order (bit-identical
+// FP32). Requires B->n <= 2^24 (see bin_of).
+template <int PL, bool NUMERIC, typename V>
+__global__ void __launch_bounds__(kSgBlock) sg_reg(const int *__restrict__ rows, int nrows, Mat A, Mat B,
+                                                   int *cnt, const int *__restrict__ crp, int *cci, V *cval) {
+    constexpr int N = 32 * PL;
+    constexpr int QB = PL == 1 ? 5 : (PL == 2 ? 6 : 7);
+    constexpr unsigned QMASK = (1u << QB) - 1u;
+    constexpr unsigned PAD = 0xffffffffu;
+    using S = RegTierSmem<PL, V>;
     __shared__ S smem[kSgBlock / 32];
     const int lane = threadIdx.x & 31;
     S &sm = smem[threadIdx.x >> 5];
@@ -137,43 +182,44 @@ __global__ void __launch_bounds__(kSgBlock) sg_warp(const int *__restrict__ rows
     const V *bval = static_cast<const V *>(B.val);
     for (int w = warp; w < nrows; w += nwarps) {
         const int i = rows[w];
-        const int rA = A.rp[i];
-        const int degA = A.rp[i + 1] - rA;  // <= UB by binning
-        for (int t = lane; t < degA; t += 32) {
-            const int k = A.ci[rA + t];
-            const int b0 = B.rp[k];
-            sm.sk_rs[t] = b0;
-            sm.soff[t] = B.rp[k + 1] - b0;
-            if (NUMERIC) sm.sa[t] = aval[rA + t];
+        const int rA = __ldg(A.rp + i);
+        const int degA = __ldg(A.rp + i + 1) - rA;  // <= N by binning
+        // A entries: B row start and length, A value
+        int len[PL];
+#pragma unroll
+        for (int r = 0; r < PL; ++r) {
+            const int t = r * 32 + lane;
+            len[r] = 0;
+            if (t < degA) {
+                const int k = __ldg(A.ci + rA + t);
+                const int b0 = __ldg(B.rp + k);
+                len[r] = __ldg(B.rp + k + 1) - b0;
+                sm.bs[t] = b0;
+                if (NUMERIC) sm.av[t] = aval[rA + t];
+            }
         }
-        for (int s = lane; s < TS; s += 32) {
-            sm.keys[s] = kEmptyKey;
-            if (NUMERIC) sm.vals[s] = V(0);
-        }
-        __syncwarp();
         int carry = 0;
-        for (int base = 0; base < degA; base += 32) {
-            const int t = base + lane;
-            const int x = t < degA ? sm.soff[t] : 0;
-            int incl = x;
+#pragma unroll
+        for (int r = 0; r < PL; ++r) {
+            int incl = len[r];
+#pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
-            if (t < degA) sm.soff[t] = carry + incl - x;
+            const int t = r * 32 + lane;
+            if (t < degA) sm.soff[t] = carry + incl - len[r];
             carry += __shfl_sync(0xffffffffu, incl, 31);
         }
-        const int ub = carry;  // <= UB by binning
+        const int ub = carry;  // <= N by binning
         if (lane == 0) sm.soff[degA] = ub;
         __syncwarp();
-        int pc[PL], pt[PL];
-        V pv[PL];
+        // gather the products and build the keys
+        unsigned key[PL];
 #pragma unroll
         for (int r = 0; r < PL; ++r) {
             const int q = r * 32 + lane;
-            pc[r] = 0;
-            pt[r] = -1;
-            pv[r] = V(0);
+            key[r] = PAD;
             if (q < ub) {
                 int lo = 0, hi = degA;  // last t with soff[t] <= q
                 while (hi - lo > 1) {
@@ -183,92 +229,79 @@ __global__ void __launch_bounds__(kSgBlock) sg_warp(const int *__restrict__ rows
                     else
                         hi = mid;
                 }
-                const int e = sm.sk_rs[lo] + (q - sm.soff[lo]);
-                pc[r] = B.ci[e];
-                pt[r] = lo;
-                if (NUMERIC) pv[r] = vmul<V>(sm.sa[lo], bval[e]);
+                const int e = sm.bs[lo] + (q - sm.soff[lo]);
+                key[r] = (static_cast<unsigned>(__ldg(B.ci + e)) << QB) | static_cast<unsigned>(q);
+                if (NUMERIC) sm.pv[q] = vmul<V>(sm.av[lo], bval[e]);
             }
         }
-        int fresh = 0;
+        // bitonic sort of the N keys, element index r * 32 + lane
+#pragma unroll
+        for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                if (j >= 32) {
+#pragma unroll
+                    for (int r = 0; r < PL; ++r) {
+                        const int p = r ^ (j >> 5);
+                        if (p > r) {
+                            const bool up = (((r * 32) & k) == 0);
+                            const unsigned a = key[r], b = key[p];
+                            if ((a > b) == up) {
+                                key[r] = b;
+                                key[p] = a;
+                            }
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < PL; ++r) {
+                        const unsigned other = __shfl_xor_sync(0xffffffffu, key[r], j);
+                        const bool up = (((r * 32 + lane) & k) == 0);
+                        const bool lower = (lane & j) == 0;
+                        key[r] = (lower == up) ? min(key[r], other) : max(key[r], other);
+                    }
+                }
+            }
+        }
+        // run heads: first element of each column
+        bool head[PL];
+        unsigned hmask[PL];
+        int count = 0;
 #pragma unroll
         for (int r = 0; r < PL; ++r) {
-            const int q0 = r * 32;
-            if (q0 >= ub) break;
-            const int last = (ub - 1 - q0) < 31 ? (ub - 1 - q0) : 31;
-            const int t_lo = __shfl_sync(0xffffffffu, pt[r], 0);
-            const int t_hi = __shfl_sync(0xffffffffu, pt[r], last);
-            for (int t = t_lo; t <= t_hi; ++t) {
-                if (pt[r] == t) {
-                    unsigned s = hash_slot(pc[r], LOG2TS);
-                    int probes = 0;
-                    for (;;) {
-                        const int k = sm.keys[s];
-                        if (k == pc[r]) break;
-                        if (k == kEmptyKey) {
-                            const int old = atomicCAS(&sm.keys[s], kEmptyKey, pc[r]);
-                            if (old == kEmptyKey) {
-                                ++fresh;
-                                break;
-                            }
-                            if (old == pc[r]) break;
-                        }
-                        s = (s + 1) & (TS - 1);
-                        if (++probes > TS) {
-                            atomicOr(&info->overflow, 1);
-                            break;
-                        }
-                    }
-                    if (NUMERIC) sm.vals[s] = vadd<V>(sm.vals[s], pv[r]);
-                }
-                __syncwarp();
+            unsigned prev = __shfl_up_sync(0xffffffffu, key[r], 1);
+            if (r > 0) {
+                const unsigned last = __shfl_sync(0xffffffffu, key[r - 1], 31);
+                if (lane == 0) prev = last;
             }
+            head[r] = key[r] != PAD && ((r == 0 && lane == 0) || (prev >> QB) != (key[r] >> QB));
+            hmask[r] = __ballot_sync(0xffffffffu, head[r]);
+            count += __popc(hmask[r]);
         }
         if (!NUMERIC) {
-            for (int o = 16; o; o >>= 1) fresh += __shfl_down_sync(0xffffffffu, fresh, o);
-            if (lane == 0) cnt[i] = fresh;
-            __syncwarp();
+            if (lane == 0) cnt[i] = count;
             continue;
         }
-        // compact the table (slot order), then bitonic-sort by column
-        const int c0 = crp[i];
-        const int nrow = crp[i + 1] - c0;
-        int pos = 0;
-        for (int s0 = 0; s0 < TS; s0 += 32) {
-            const int k = sm.keys[s0 + lane];
-            const bool v = k != kEmptyKey;
-            const unsigned mask = __ballot_sync(0xffffffffu, v);
-            if (v) {
-                const int p = pos + __popc(mask & ((1u << lane) - 1u));
-                if (p < UB) {
-                    sm.lk[p] = k;
-                    sm.lv[p] = sm.vals[s0 + lane];
-                }
-            }
-            pos += __popc(mask);
-        }
-        for (int p = pos + lane; p < UB; p += 32) sm.lk[p] = 0x7fffffff;
+#pragma unroll
+        for (int r = 0; r < PL; ++r) sm.skey[r * 32 + lane] = key[r];
         __syncwarp();
-        for (int k2 = 2; k2 <= UB; k2 <<= 1) {
-            for (int j = k2 >> 1; j > 0; j >>= 1) {
-                for (int idx = lane; idx < UB / 2; idx += 32) {
-                    const int a = 2 * idx - (idx & (j - 1));
-                    const int b = a + j;
-                    const bool up = (a & k2) == 0;
-                    const int ka = sm.lk[a], kb = sm.lk[b];
-                    if ((ka > kb) == up) {
-                        sm.lk[a] = kb;
-                        sm.lk[b] = ka;
-                        const V t = sm.lv[a];
-                        sm.lv[a] = sm.lv[b];
-                        sm.lv[b] = t;
-                    }
+        const int c0 = crp[i];
+        int before = 0;
+#pragma unroll
+        for (int r = 0; r < PL; ++r) {
+            if (head[r]) {
+                const int rank = before + __popc(hmask[r] & ((1u << lane) - 1u));
+                const unsigned col = key[r] >> QB;
+                V sum = sm.pv[key[r] & QMASK];
+                for (int f = r * 32 + lane + 1; f < ub; ++f) {
+                    const unsigned kf = sm.skey[f];
+                    if ((kf >> QB) != col) break;
+                    sum = vadd<V>(sum, sm.pv[kf & QMASK]);
                 }
-                __syncwarp();
+                cci[c0 + rank] = static_cast<int>(col);
+                cval[c0 + rank] = sum;
             }
-        }
-        for (int p = lane; p < nrow; p += 32) {
-            cci[c0 + p] = sm.lk[p];
-            cval[c0 + p] = sm.lv[p];
+            before += __popc(hmask[r]);
         }
         __syncwarp();
     }
@@ -468,6 +501,7 @@ struct SgPlan {
     int *gkeys;
     void *gvals;
     SgInfo *info;
+    unsigned char *row_bin;
     SgInfo h;
 };
 
@@ -491,7 +525,7 @@ apspie_status sg_plan(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B,
     const size_t mi = static_cast<size_t>(m) + 1;
     const size_t base_need =
         Carver::need({mi * 8, static_cast<size_t>(kBins) * mi * 4, mi * 8, mi * 4,
-                      scan_scratch_bytes(m) + 64, sizeof(SgInfo)});
+                      scan_scratch_bytes(m) + 64, sizeof(SgInfo), mi});
     void *base;
     apspie_status st = scratch_reserve(ctx, base_need, &base);
     if (st != APSPIE_OK) return st;
@@ -502,12 +536,16 @@ apspie_status sg_plan(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B,
     p.cnt = c.take<int>(mi);
     p.scan_tmp = c.take<char>(scan_scratch_bytes(m) + 64);
     p.info = c.take<SgInfo>(1);
+    p.row_bin = c.take<unsigned char>(mi);
     cudaError_t e = cudaMemsetAsync(p.info, 0, sizeof(SgInfo), ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "spgemm info reset");
     Mat a{A->row_ptr, A->col_ind, A->val}, b{B->row_ptr, B->col_ind, B->val};
     if (m > 0) {
-        const int blocks = std::min<long long>((static_cast<long long>(m) * 32 + 255) / 256, ctx->num_sms * 16LL);
-        sg_rowinfo<<<blocks, 256, 0, ctx->stream>>>(m, a, b, p.ub, p.bin_rows, p.info, p.tbl_off);
+        const int blocks = std::min<long long>((static_cast<long long>(m) * 8 + 255) / 256, ctx->num_sms * 16LL);
+        sg_rowinfo<<<blocks, 256, 0, ctx->stream>>>(m, a, b, B->n <= (1 << 24), p.ub, p.row_bin, p.info,
+                                                    p.tbl_off);
+        const int lblocks = std::min<long long>((static_cast<long long>(m) + 255) / 256, ctx->num_sms * 8LL);
+        sg_binlists<<<lblocks, 256, 0, ctx->stream>>>(m, p.row_bin, p.bin_rows, p.info);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "spgemm rowinfo");
     }
     e = cudaMemcpyAsync(&p.h, p.info, sizeof(SgInfo), cudaMemcpyDeviceToHost, ctx->stream);
@@ -538,31 +576,32 @@ apspie_status sg_run(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B, 
     (void)mi;
     // per-bin lists are laid out with stride m (sg_rowinfo)
     auto rows = [&](int bin) { return p.bin_rows + static_cast<long long>(bin) * m; };
+    const int reg_cap = ctx->num_sms * 16;
     int nb = p.h.bin_count[1];
-    if (nb > 0) {
-        const int g = std::min((nb + 7) / 8, grid_cap);
-        sg_warp<1, 64, 6, NUMERIC, V><<<g, kSgBlock, 0, ctx->stream>>>(rows(1), nb, a, b, p.cnt, crp, cci, cval,
-                                                                         p.info);
-    }
+    if (nb > 0)
+        sg_reg<1, NUMERIC, V><<<std::min((nb + 7) / 8, reg_cap), kSgBlock, 0, ctx->stream>>>(rows(1), nb, a, b,
+                                                                                             p.cnt, crp, cci, cval);
     nb = p.h.bin_count[2];
-    if (nb > 0) {
-        const int g = std::min((nb + 7) / 8, grid_cap);
-        sg_warp<4, 256, 8, NUMERIC, V><<<g, kSgBlock, 0, ctx->stream>>>(rows(2), nb, a, b, p.cnt, crp, cci, cval,
-                                                                          p.info);
-    }
+    if (nb > 0)
+        sg_reg<2, NUMERIC, V><<<std::min((nb + 7) / 8, reg_cap), kSgBlock, 0, ctx->stream>>>(rows(2), nb, a, b,
+                                                                                             p.cnt, crp, cci, cval);
     nb = p.h.bin_count[3];
+    if (nb > 0)
+        sg_reg<4, NUMERIC, V><<<std::min((nb + 7) / 8, reg_cap), kSgBlock, 0, ctx->stream>>>(rows(3), nb, a, b,
+                                                                                             p.cnt, crp, cci, cval);
+    nb = p.h.bin_count[kBinBlock];
     if (nb > 0) {
         const int g = std::min(nb, grid_cap);
-        sg_block<false, NUMERIC, V><<<g, kSgBlock, 0, ctx->stream>>>(rows(3), nb, a, b, p.ub, p.tbl_off, p.gkeys,
-                                                                      static_cast<V *>(p.gvals), p.cnt, crp, cci,
-                                                                      cval, p.info);
+        sg_block<false, NUMERIC, V><<<g, kSgBlock, 0, ctx->stream>>>(rows(kBinBlock), nb, a, b, p.ub, p.tbl_off,
+                                                                      p.gkeys, static_cast<V *>(p.gvals), p.cnt,
+                                                                      crp, cci, cval, p.info);
     }
-    nb = p.h.bin_count[4];
+    nb = p.h.bin_count[kBinGlobal];
     if (nb > 0) {
         const int g = std::min(nb, grid_cap);
-        sg_block<true, NUMERIC, V><<<g, kSgBlock, 0, ctx->stream>>>(rows(4), nb, a, b, p.ub, p.tbl_off, p.gkeys,
-                                                                     static_cast<V *>(p.gvals), p.cnt, crp, cci,
-                                                                     cval, p.info);
+        sg_block<true, NUMERIC, V><<<g, kSgBlock, 0, ctx->stream>>>(rows(kBinGlobal), nb, a, b, p.ub, p.tbl_off,
+                                                                     p.gkeys, static_cast<V *>(p.gvals), p.cnt,
+                                                                     crp, cci, cval, p.info);
     }
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? APSPIE_OK : cuda_error(ctx, e, "spgemm launch");
@@ -611,6 +650,50 @@ apspie_status sg_numeric(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr 
     return st;
 }
 
+bool same_view(const apspie_csr &x, const apspie_csr *y) {
+    return x.m == y->m && x.n == y->n && x.nnz == y->nnz && x.val_type == y->val_type &&
+           x.row_ptr == y->row_ptr && x.col_ind == y->col_ind && x.val == y->val;
+}
+
+// The validation pass (ctx->validate) reserves no scratch, so it leaves the epoch alone.
+void sg_cache_store(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B, const SgPlan &p) {
+    apspie_spgemm_plan_cache &c = ctx->sg_cache;
+    c.a = *A;
+    c.b = *B;
+    c.dev[0] = p.ub;
+    c.dev[1] = p.bin_rows;
+    c.dev[2] = p.tbl_off;
+    c.dev[3] = p.cnt;
+    c.dev[4] = p.scan_tmp;
+    c.dev[5] = p.gkeys;
+    c.dev[6] = p.gvals;
+    c.dev[7] = p.info;
+    static_assert(kBins <= 8, "cache layout");
+    for (int b = 0; b < kBins; ++b) c.host[b] = p.h.bin_count[b];
+    c.host[8] = p.h.global_slots;
+    c.host[9] = reinterpret_cast<long long>(p.row_bin);
+    c.epoch = ctx->scratch_epoch;
+    c.valid = true;
+}
+
+bool sg_cache_load(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B, SgPlan &p) {
+    const apspie_spgemm_plan_cache &c = ctx->sg_cache;
+    if (!c.valid || c.epoch != ctx->scratch_epoch || !same_view(c.a, A) || !same_view(c.b, B)) return false;
+    p.ub = static_cast<long long *>(c.dev[0]);
+    p.bin_rows = static_cast<int *>(c.dev[1]);
+    p.tbl_off = static_cast<long long *>(c.dev[2]);
+    p.cnt = static_cast<int *>(c.dev[3]);
+    p.scan_tmp = c.dev[4];
+    p.gkeys = static_cast<int *>(c.dev[5]);
+    p.gvals = c.dev[6];
+    p.info = static_cast<SgInfo *>(c.dev[7]);
+    std::memset(&p.h, 0, sizeof(p.h));
+    for (int b = 0; b < kBins; ++b) p.h.bin_count[b] = static_cast<int>(c.host[b]);
+    p.h.global_slots = c.host[8];
+    p.row_bin = reinterpret_cast<unsigned char *>(c.host[9]);
+    return true;
+}
+
 }  // namespace
 }  // namespace apspie
 
@@ -622,6 +705,7 @@ apspie_status apspie_spgemm_symbolic(apspie_ctx *ctx, const apspie_csr *A, const
                                      int32_t *d_row_ptr_c, int64_t *nnz_c) {
     if (!ctx || !d_row_ptr_c || !nnz_c) return APSPIE_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
+    ctx->sg_cache.valid = false;
     apspie_status st = check_pair(ctx, A, B, "apspie_spgemm_symbolic");
     if (st != APSPIE_OK) return st;
     SgPlan p;
@@ -629,6 +713,7 @@ apspie_status apspie_spgemm_symbolic(apspie_ctx *ctx, const apspie_csr *A, const
     long long nnz = 0;
     if ((st = sg_symbolic(ctx, A, B, p, d_row_ptr_c, &nnz)) != APSPIE_OK) return st;
     *nnz_c = nnz;
+    sg_cache_store(ctx, A, B, p);
     return APSPIE_OK;
 }
 
@@ -639,7 +724,7 @@ apspie_status apspie_spgemm_numeric(apspie_ctx *ctx, const apspie_csr *A, const 
     apspie_status st = check_pair(ctx, A, B, "apspie_spgemm_numeric");
     if (st != APSPIE_OK) return st;
     SgPlan p;
-    if ((st = sg_plan(ctx, A, B, p)) != APSPIE_OK) return st;
+    if (!sg_cache_load(ctx, A, B, p) && (st = sg_plan(ctx, A, B, p)) != APSPIE_OK) return st;
     return sg_numeric(ctx, A, B, p, d_row_ptr_c, d_col_c, d_val_c);
 }
 
