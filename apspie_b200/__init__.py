@@ -3,7 +3,8 @@
 The product is the C-ABI shared library built from ``apspie_b200/csrc`` (declared in
 ``include/apspie.h``); this package loads it with ctypes for tests and benchmarks.
 """
-from ._lib import ApspieError, ApspieLibraryMissing, LIB_PATH, VAL_F32, VAL_I32, VAL_NONE, lib
+from ._lib import (ApspieError, ApspieLibraryMissing, LIB_PATH, TUNE_BFS, TUNE_BFS_BATCH, TUNE_SPGEMM, TUNE_SSSP,
+                   TUNE_TC, VAL_F32, VAL_I32, VAL_NONE, lib)
 from .graph import (
     Context,
     DeviceGraph,
@@ -20,6 +21,7 @@ from .graph import (
 
 __all__ = [
     "ApspieError", "ApspieLibraryMissing", "LIB_PATH", "VAL_F32", "VAL_I32", "VAL_NONE", "lib",
+    "TUNE_BFS", "TUNE_SSSP", "TUNE_BFS_BATCH", "TUNE_SPGEMM", "TUNE_TC",
     "Context", "DeviceGraph", "HostGraph", "Server", "gen_er", "gen_rmat", "lcc_sample", "load_mtx",
     "max_degree_vertex", "mt19937_u32", "strict_lower",
 ]

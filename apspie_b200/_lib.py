@@ -73,6 +73,17 @@ class RunStats(ctypes.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
 
 
+class TuneParams(ctypes.Structure):
+    _fields_ = [
+        ("bfs_alpha", c_float), ("bfs_beta", c_float), ("batch_push_frac", c_float), ("sssp_delta", c_int32),
+        ("sssp_band", c_int64), ("spgemm_reg_max", c_int32), ("spgemm_block_max", c_int32),
+        ("tc_task_work", c_int32), ("tc_orient", c_int32), ("reserved", c_int32 * 4),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, c_int64) for n in ("submitted", "completed", "failed", "launches", "batched_queries",
                                         "max_batch_seen", "deferred", "peak_bytes", "resident_bytes")]
@@ -82,6 +93,7 @@ class ServerStats(ctypes.Structure):
 
 
 QUERY_BFS, QUERY_SSSP, QUERY_MIS = 0, 1, 2
+TUNE_BFS, TUNE_SSSP, TUNE_BFS_BATCH, TUNE_SPGEMM, TUNE_TC = 0, 1, 2, 3, 4
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -95,6 +107,15 @@ SIGNATURES = {
     "apspie_ctx_set_bfs_tuning": (c_int, [c_void_p, c_float, c_float]),
     "apspie_ctx_set_sssp_delta": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_set_sssp_band": (c_int, [c_void_p, c_int64]),
+    "apspie_ctx_get_params": (c_int, [c_void_p, POINTER(TuneParams)]),
+    "apspie_ctx_set_params": (c_int, [c_void_p, POINTER(TuneParams)]),
+    "apspie_ctx_set_autotune": (c_int, [c_void_p, c_int32]),
+    "apspie_autotune": (c_int, [c_void_p, c_int32, c_void_p, c_void_p, POINTER(c_int32), c_int32, c_int32,
+                                POINTER(TuneParams), POINTER(c_double)]),
+    "apspie_tune_entries": (c_int32, [c_void_p]),
+    "apspie_tune_lookup": (c_int, [c_void_p, c_int32, c_void_p, POINTER(TuneParams), POINTER(c_int32)]),
+    "apspie_tune_save": (c_int, [c_void_p, c_char_p]),
+    "apspie_tune_load": (c_int, [c_void_p, c_char_p]),
     "apspie_ctx_set_max_grid": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_set_batch_push_frac": (c_int, [c_void_p, c_float]),
     "apspie_ctx_scratch_bytes": (c_int64, [c_void_p]),

@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/apspie.h"
 
@@ -64,6 +65,13 @@ struct apspie_spgemm_plan_cache {
     long long host[12] = {};  // bin counts and sizes read back at planning
 };
 
+// One tuning-table entry: the knobs the autotuner chose for a (kind, shape bucket).
+struct apspie_tune_entry {
+    int kind, log_m, log_deg, symmetric;
+    apspie_tune_params p;
+    double ms;
+};
+
 struct apspie_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -89,6 +97,12 @@ struct apspie_ctx {
     long long sssp_band = 0;  // 0: auto, < 0: off
     int max_grid = 0;    // 0: as many co-resident blocks as fit
     float batch_push_frac = 0.05f;  // batched BFS: push while frontier edges < frac * nnz
+    int spgemm_reg_max = 128;       // SpGEMM register tier: rows of <= this many products
+    int spgemm_block_max = 1024;    // SpGEMM shared-table tier: rows of <= this many products
+    int tc_task_work = 4096;        // TC wedges per warp task
+    int tc_orient = 1;              // TC: re-orient L by degree
+    int use_tuning = 1;             // consult tune_table
+    std::vector<apspie_tune_entry> tune_table;
 };
 
 namespace apspie {
@@ -98,6 +112,9 @@ namespace apspie {
 // ---------------------------------------------------------------------------------
 apspie_status set_error(apspie_ctx *ctx, apspie_status st, const std::string &msg);
 apspie_status cuda_error(apspie_ctx *ctx, cudaError_t e, const char *what);
+// The knobs a call of `kind` on A uses: the context's own, overridden by its tuning-table
+// entry for A's shape bucket when there is one (and use_tuning is on).
+apspie_tune_params effective_params(const apspie_ctx *ctx, int kind, const apspie_csr *A);
 // Ensures the arena holds `bytes`; returns its base in *out.
 apspie_status scratch_reserve(apspie_ctx *ctx, size_t bytes, void **out);
 apspie_status scratch2_reserve(apspie_ctx *ctx, size_t bytes, void **out);

@@ -459,7 +459,9 @@ extern "C" apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, 
         a.ctl = ctx->d_ctl;
         a.sticky = ctx->d_sticky_err;
         // pull levels scan a vertex's own row for parents: valid for symmetric patterns only
-        a.push_frac = (A->flags & APSPIE_CSR_SYMMETRIC) ? ctx->batch_push_frac : 1e30f;
+        a.push_frac = (A->flags & APSPIE_CSR_SYMMETRIC)
+                          ? effective_params(ctx, APSPIE_TUNE_BFS_BATCH, A).batch_push_frac
+                          : 1e30f;
         cudaError_t e = cudaMemsetAsync(a.out, 0xff, static_cast<size_t>(nq) * m * sizeof(int32_t), ctx->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(TravCtl), ctx->stream);
         if (e != cudaSuccess) return cuda_error(ctx, e, "apspie_bfs_batch reset");

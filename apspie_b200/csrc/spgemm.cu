@@ -48,16 +48,16 @@ struct SgInfo {
     long long global_slots;
 };
 
-// reg_ok: B has at most 2^24 columns, so a register-tier key (column << 7 | product)
-// stays below the padding key 0xffffffff.
-__device__ __forceinline__ int bin_of(long long ub, int degA, bool reg_ok) {
+// Rows of at most reg_max products (0, 32, 64 or 128) go to the register tiers (needs B
+// with at most 2^24 columns, so that a key column << 7 | product stays below the padding
+// key 0xffffffff; the host passes reg_max 0 otherwise), rows of at most block_max (<= 1024,
+// the shared table holds 2048 slots) to the shared-memory table, longer rows to a global
+// table.
+__device__ __forceinline__ int bin_of(long long ub, int degA, int reg_max, int block_max) {
     const long long w = ub > degA ? ub : degA;
     if (ub == 0) return 0;
-    if (!reg_ok && w <= 1024) return kBinBlock;
-    if (w <= 32) return 1;
-    if (w <= 64) return 2;
-    if (w <= 128) return 3;
-    if (w <= 1024) return kBinBlock;
+    if (w <= reg_max) return w <= 32 ? 1 : (w <= 64 ? 2 : 3);
+    if (w <= block_max) return kBinBlock;
     return kBinGlobal;
 }
 
@@ -86,8 +86,8 @@ struct Mat {
 
 // ---------------------------------------------------------------- 1. row info / bins
 // 8 lanes per row: ub = sum of deg_B over A's row, and the row's bin.
-__global__ void sg_rowinfo(int m, Mat A, Mat B, bool reg_ok, long long *ub, unsigned char *row_bin,
-                           SgInfo *info, long long *tbl_off) {
+__global__ void sg_rowinfo(int m, Mat A, Mat B, int reg_max, int block_max, long long *ub,
+                           unsigned char *row_bin, SgInfo *info, long long *tbl_off) {
     const int sub = threadIdx.x & 7;
     const int grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
     const int ngrp = (gridDim.x * blockDim.x) >> 3;
@@ -107,7 +107,7 @@ __global__ void sg_rowinfo(int m, Mat A, Mat B, bool reg_ok, long long *ub, unsi
         for (int o = 4; o; o >>= 1) s += __shfl_down_sync(gmask, s, o, 8);
         if (i < m && sub == 0) {
             ub[i] = s;
-            const int b = bin_of(s, r1 - r0, reg_ok);
+            const int b = bin_of(s, r1 - r0, reg_max, block_max);
             row_bin[i] = static_cast<unsigned char>(b);
             if (b == kBinGlobal) {
                 long long ts = 64;
@@ -542,8 +542,10 @@ apspie_status sg_plan(apspie_ctx *ctx, const apspie_csr *A, const apspie_csr *B,
     Mat a{A->row_ptr, A->col_ind, A->val}, b{B->row_ptr, B->col_ind, B->val};
     if (m > 0) {
         const int blocks = std::min<long long>((static_cast<long long>(m) * 8 + 255) / 256, ctx->num_sms * 16LL);
-        sg_rowinfo<<<blocks, 256, 0, ctx->stream>>>(m, a, b, B->n <= (1 << 24), p.ub, p.row_bin, p.info,
-                                                    p.tbl_off);
+        const apspie_tune_params tp = effective_params(ctx, APSPIE_TUNE_SPGEMM, A);
+        const int reg_max = B->n <= (1 << 24) ? tp.spgemm_reg_max : 0;
+        sg_rowinfo<<<blocks, 256, 0, ctx->stream>>>(m, a, b, reg_max, tp.spgemm_block_max, p.ub, p.row_bin,
+                                                    p.info, p.tbl_off);
         const int lblocks = std::min<long long>((static_cast<long long>(m) + 255) / 256, ctx->num_sms * 8LL);
         sg_binlists<<<lblocks, 256, 0, ctx->stream>>>(m, p.row_bin, p.bin_rows, p.info);
         if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "spgemm rowinfo");

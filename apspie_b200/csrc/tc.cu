@@ -13,11 +13,11 @@
 // under L, 0.66G under D, largest row 8,083 -> 411). Each row i of D is loaded into a hash
 // set (its mask); every wedge (k in D(i,:), j in D(k,:)) probes the set, and hits are
 // counted in int64. Rows with masks of at most 256 entries are cut into warp tasks of at
-// most kTaskWork wedges (each task loads its row's mask into a 512-slot shared-memory set,
-// so skewed rows cannot unbalance the warps); larger masks take a block with a 4096-slot
-// shared set, or a block with a global set. An input with an entry on or above the
-// diagonal is not a strict lower triangle; it is counted as given, sum((L*L) .* L),
-// without re-orientation.
+// most task_work wedges (4096 unless tuned); each task loads its row's mask into a
+// 512-slot shared-memory set, so skewed rows cannot unbalance the warps. Larger masks
+// take a block with a 4096-slot shared set, or a block with a global set. An input with
+// an entry on or above the diagonal is not a strict lower triangle; it is counted as
+// given, sum((L*L) .* L), without re-orientation (also when orientation is tuned off).
 #include <algorithm>
 #include <cstring>
 
@@ -31,7 +31,6 @@ constexpr int kEmpty = -1;
 constexpr int kTcBins = 4;        // 0 nothing to do | 1 warp | 2 block/shared | 3 block/global
 constexpr int kWarpSet = 512;     // slots (mask <= 256)
 constexpr int kBlockSet = 4096;   // slots (mask <= 2048)
-constexpr int kTaskWork = 4096;    // wedges per warp task (a warp-tier row is split in tasks)
 
 struct TcInfo {
     int bin_count[kTcBins];
@@ -46,8 +45,8 @@ __device__ __forceinline__ unsigned tc_hash(int key, int log2ts) {
 }
 
 // 8 lanes per row: mask size d and wedge count; the row's bin goes to row_bin and, for a
-// warp-tier row, its number of warp tasks (kTaskWork wedges each) to ntask.
-__global__ void tc_rowinfo(int m, const int *__restrict__ rp, const int *__restrict__ ci,
+// warp-tier row, its number of warp tasks (task_work wedges each) to ntask.
+__global__ void tc_rowinfo(int m, const int *__restrict__ rp, const int *__restrict__ ci, int task_work,
                            unsigned char *row_bin, int *ntask, long long *tbl_off, TcInfo *info) {
     const int sub = threadIdx.x & 7;
     const int grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
@@ -79,7 +78,7 @@ __global__ void tc_rowinfo(int m, const int *__restrict__ rp, const int *__restr
             else
                 b = 3;
             row_bin[i] = static_cast<unsigned char>(b);
-            ntask[i] = b == 1 ? static_cast<int>((work + kTaskWork - 1) / kTaskWork) : 0;
+            ntask[i] = b == 1 ? static_cast<int>((work + task_work - 1) / task_work) : 0;
             if (b == 3) {
                 long long ts = 64;
                 while (ts < 2LL * d) ts <<= 1;
@@ -206,12 +205,12 @@ struct TcWarpSmem {
 };
 
 // Warp tasks: task t belongs to the row r with task_ptr[r] <= t < task_ptr[r + 1] and
-// covers wedges [c * kTaskWork, (c + 1) * kTaskWork) of it, c = t - task_ptr[r]. Each task
+// covers wedges [c * task_work, (c + 1) * task_work) of it, c = t - task_ptr[r]. Each task
 // loads its row's mask (<= 256 entries) into its warp's set, so tasks are independent and
 // of bounded size, and warps stay balanced however skewed the rows are.
 __global__ void __launch_bounds__(kTcBlock) tc_warp(const int *__restrict__ task_ptr, int m, int ntasks,
-                                                    const int *__restrict__ rp, const int *__restrict__ ci,
-                                                    TcInfo *info) {
+                                                    int task_work, const int *__restrict__ rp,
+                                                    const int *__restrict__ ci, TcInfo *info) {
     __shared__ TcWarpSmem smem[kTcBlock / 32];
     const int lane = threadIdx.x & 31;
     TcWarpSmem &sm = smem[threadIdx.x >> 5];
@@ -230,7 +229,7 @@ __global__ void __launch_bounds__(kTcBlock) tc_warp(const int *__restrict__ task
                 hi = mid;
         }
         const int i = lo;
-        const int w0 = (t - __ldg(task_ptr + i)) * kTaskWork;
+        const int w0 = (t - __ldg(task_ptr + i)) * task_work;
         const int r0 = __ldg(rp + i);
         const int d = __ldg(rp + i + 1) - r0;
         for (int s = lane; s < kWarpSet; s += 32) sm.keys[s] = kEmpty;
@@ -262,7 +261,7 @@ __global__ void __launch_bounds__(kTcBlock) tc_warp(const int *__restrict__ task
         }
         if (lane == 0) sm.soff[nv] = carry;
         __syncwarp();
-        const int w1 = min(carry, w0 + kTaskWork);
+        const int w1 = min(carry, w0 + task_work);
         // o0: the listed row holding wedge w0 (last with soff <= w0)
         int o0 = 0;
         {
@@ -440,7 +439,8 @@ apspie_status apspie_tc(apspie_ctx *ctx, const apspie_csr *L, int64_t *count) {
     if (e != cudaSuccess) return cuda_error(ctx, e, "tc reset");
     const int wblocks = std::max(1, std::min<int>((m * 32LL + 255) / 256, ctx->num_sms * 16));
     const int *rp = L->row_ptr, *ci = L->col_ind;
-    if (m > 0) {
+    const apspie_tune_params tp = effective_params(ctx, APSPIE_TUNE_TC, L);
+    if (m > 0 && tp.tc_orient) {
         // D: L's edges oriented from lower to higher (degree, id) rank
         tc_degree<<<wblocks, 256, 0, ctx->stream>>>(m, rp, ci, deg, info);
         tc_orient<0><<<wblocks, 256, 0, ctx->stream>>>(m, rp, ci, deg, ocnt, nullptr, nullptr);
@@ -456,7 +456,8 @@ apspie_status apspie_tc(apspie_ctx *ctx, const apspie_csr *L, int64_t *count) {
     int ntasks = 0;
     for (int attempt = 0; attempt < 2; ++attempt) {
         if (m > 0) {
-            tc_rowinfo<<<rblocks, 256, 0, ctx->stream>>>(m, rp, ci, row_bin, ntask, tbl_off, info);
+            tc_rowinfo<<<rblocks, 256, 0, ctx->stream>>>(m, rp, ci, tp.tc_task_work, row_bin, ntask, tbl_off,
+                                                         info);
             tc_binlists<<<lblocks, 256, 0, ctx->stream>>>(m, row_bin, bin_rows, info);
             if ((st = device_exclusive_scan(ctx, ntask, m, task_ptr, stmp, &info->overflow)) != APSPIE_OK) return st;
             if ((e = cudaMemcpyAsync(&ntasks, task_ptr + m, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream)) !=
@@ -466,7 +467,7 @@ apspie_status apspie_tc(apspie_ctx *ctx, const apspie_csr *L, int64_t *count) {
         if ((e = cudaMemcpyAsync(&h, info, sizeof(TcInfo), cudaMemcpyDeviceToHost, ctx->stream)) != cudaSuccess ||
             (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
             return cuda_error(ctx, e, "tc plan");
-        if (!h.not_lower || attempt == 1) break;
+        if (!h.not_lower || attempt == 1 || !tp.tc_orient) break;
         // not a strict lower triangle: count sum((L*L) .* L) on L as given
         rp = L->row_ptr;
         ci = L->col_ind;
@@ -482,7 +483,8 @@ apspie_status apspie_tc(apspie_ctx *ctx, const apspie_csr *L, int64_t *count) {
     }
     const int cap = ctx->num_sms * 8;
     if (ntasks > 0)
-        tc_warp<<<std::min((ntasks + 7) / 8, cap), kTcBlock, 0, ctx->stream>>>(task_ptr, m, ntasks, rp, ci, info);
+        tc_warp<<<std::min((ntasks + 7) / 8, cap), kTcBlock, 0, ctx->stream>>>(task_ptr, m, ntasks,
+                                                                                 tp.tc_task_work, rp, ci, info);
     if (h.bin_count[2] > 0)
         tc_block<false><<<std::min(h.bin_count[2], cap), kTcBlock, 0, ctx->stream>>>(
             bin_rows + 2 * static_cast<size_t>(m), h.bin_count[2], rp, ci, tbl_off, gkeys, info);

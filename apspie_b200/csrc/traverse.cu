@@ -974,8 +974,9 @@ apspie_status apspie_bfs(apspie_ctx *ctx, const apspie_csr *A, int32_t source, i
     a.buf = carve_trav(base, A->m);
     a.ctl = ctx->d_ctl;
     a.sticky = ctx->d_sticky_err;
-    a.alpha = ctx->bfs_alpha;
-    a.beta = ctx->bfs_beta;
+    const apspie_tune_params tp = effective_params(ctx, APSPIE_TUNE_BFS, A);
+    a.alpha = tp.bfs_alpha;
+    a.beta = tp.bfs_beta;
     a.allow_pull = (A->flags & APSPIE_CSR_SYMMETRIC) ? 1 : 0;
     void *args[] = {&a};
     st = launch_persistent(ctx, reinterpret_cast<const void *>(bfs_kernel), kBlock, args, A->nnz);
@@ -1033,10 +1034,11 @@ apspie_status sssp_common(apspie_ctx *ctx, const apspie_csr *A, int32_t source, 
     a.col_ind = A->col_ind;
     a.w = static_cast<const int *>(A->val);
     a.dist = static_cast<int *>(d_dist);
-    a.delta_hint = ctx->sssp_delta;
-    if (ctx->sssp_band > 0) {
-        a.band = ctx->sssp_band;
-    } else if (ctx->sssp_band == 0) {
+    const apspie_tune_params tp = effective_params(ctx, APSPIE_TUNE_SSSP, A);
+    a.delta_hint = tp.sssp_delta;
+    if (tp.sssp_band > 0) {
+        a.band = tp.sssp_band;
+    } else if (tp.sssp_band == 0) {
         const long long b = A->nnz / 8;
         a.band = b < (1LL << 18) ? (1LL << 18) : (b > (1LL << 23) ? (1LL << 23) : b);
     } else {

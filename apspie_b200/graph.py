@@ -218,6 +218,53 @@ class Context:
         """Edges expanded per SSSP iteration (lowest-distance band); 0 = auto, < 0 = off."""
         self._check(L.lib().apspie_ctx_set_sssp_band(self.handle, edges), "set_sssp_band")
 
+    # ---- autotuner
+    def get_params(self) -> dict:
+        p = L.TuneParams()
+        self._check(L.lib().apspie_ctx_get_params(self.handle, ctypes.byref(p)), "get_params")
+        return p.as_dict()
+
+    def set_params(self, **knobs) -> None:
+        """Sets some of the context's own knobs (names as in apspie_tune_params)."""
+        p = L.TuneParams()
+        self._check(L.lib().apspie_ctx_get_params(self.handle, ctypes.byref(p)), "get_params")
+        for k, v in knobs.items():
+            setattr(p, k, v)
+        self._check(L.lib().apspie_ctx_set_params(self.handle, ctypes.byref(p)), "set_params")
+
+    def set_autotune(self, use: bool) -> None:
+        self._check(L.lib().apspie_ctx_set_autotune(self.handle, 1 if use else 0), "set_autotune")
+
+    def autotune(self, kind: int, A: DeviceGraph, B: DeviceGraph = None, sources=None, reps: int = 3):
+        """Times the candidates of `kind` on this input; returns (chosen knobs, median ms)."""
+        best = L.TuneParams()
+        ms = ctypes.c_double()
+        src = None
+        n = 0
+        if sources is not None:
+            arr = (ctypes.c_int32 * len(sources))(*[int(x) for x in sources])
+            src, n = arr, len(sources)
+        self._check(L.lib().apspie_autotune(self.handle, kind, ctypes.byref(A.view(True)),
+                                            ctypes.byref(B.view(True)) if B is not None else None,
+                                            src, n, reps, ctypes.byref(best), ctypes.byref(ms)), "autotune")
+        return best.as_dict(), ms.value
+
+    def tune_entries(self) -> int:
+        return int(L.lib().apspie_tune_entries(self.handle))
+
+    def tune_lookup(self, kind: int, A: DeviceGraph):
+        p = L.TuneParams()
+        found = ctypes.c_int32()
+        self._check(L.lib().apspie_tune_lookup(self.handle, kind, ctypes.byref(A.view(False)), ctypes.byref(p),
+                                               ctypes.byref(found)), "tune_lookup")
+        return p.as_dict(), bool(found.value)
+
+    def tune_save(self, path: str) -> None:
+        self._check(L.lib().apspie_tune_save(self.handle, str(path).encode()), "tune_save")
+
+    def tune_load(self, path: str) -> None:
+        self._check(L.lib().apspie_tune_load(self.handle, str(path).encode()), "tune_load")
+
     def set_batch_push_frac(self, frac: float) -> None:
         self._check(L.lib().apspie_ctx_set_batch_push_frac(self.handle, frac), "set_batch_push_frac")
 

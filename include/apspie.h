@@ -129,6 +129,59 @@ apspie_status apspie_ctx_timeline(const apspie_ctx *ctx, int32_t *sites, int64_t
 /* Bytes of device scratch the context currently holds. */
 int64_t apspie_ctx_scratch_bytes(const apspie_ctx *ctx);
 
+/* ---- autotuner ------------------------------------------------------------------ */
+
+/* The knobs the autotuner picks. A context holds one set of its own (the set_* calls
+ * above and apspie_ctx_set_params) and a tuning table of sets recorded per (kind, shape
+ * bucket); a call whose input falls in a recorded bucket uses the recorded set for the
+ * knobs of its kind (unless apspie_ctx_set_autotune(ctx, 0)). No reference counterpart:
+ * the reference's thresholds are compile-time constants. */
+typedef struct apspie_tune_params {
+    float bfs_alpha;          /* BFS push -> pull when frontier edges > unvisited edges / alpha */
+    float bfs_beta;           /* BFS pull -> push when frontier < m / beta */
+    float batch_push_frac;    /* batched BFS: push while frontier edges < frac * nnz */
+    int32_t sssp_delta;       /* SSSP far-pile step (<= 0: none with the band, else device-chosen) */
+    int64_t sssp_band;        /* SSSP edges per iteration (0 auto, < 0 whole frontier) */
+    int32_t spgemm_reg_max;   /* SpGEMM rows with at most this many products (0, 32, 64 or 128)
+                                 are sorted by one warp in registers */
+    int32_t spgemm_block_max; /* larger rows up to this many products (<= 1024) use a block's
+                                 shared-memory hash table; longer rows a global table */
+    int32_t tc_task_work;     /* triangle counting: wedges per warp task (>= 256) */
+    int32_t tc_orient;        /* triangle counting: 1 = re-orient L by degree first */
+    int32_t reserved[4];
+} apspie_tune_params;
+
+enum {
+    APSPIE_TUNE_BFS = 0,
+    APSPIE_TUNE_SSSP = 1,
+    APSPIE_TUNE_BFS_BATCH = 2,
+    APSPIE_TUNE_SPGEMM = 3,
+    APSPIE_TUNE_TC = 4
+};
+
+apspie_status apspie_ctx_get_params(const apspie_ctx *ctx, apspie_tune_params *out);
+/* Replaces the context's own knobs (validated: APSPIE_ERR_INVALID_ARG if out of range). */
+apspie_status apspie_ctx_set_params(apspie_ctx *ctx, const apspie_tune_params *p);
+/* use != 0 (default): calls consult the tuning table; 0: only the context's own knobs. */
+apspie_status apspie_ctx_set_autotune(apspie_ctx *ctx, int32_t use);
+/* Times every candidate setting of `kind`'s knobs on this input (reps timed runs each,
+ * after one warm-up; the median counts), records the fastest for the input's shape
+ * bucket and returns it in *best (and its median milliseconds in *best_ms). Inputs:
+ * BFS/SSSP: A and host `sources[0]`; BFS_BATCH: A and `nsources` host sources; SPGEMM:
+ * A and B; TC: A = strict lower triangle. Output buffers are allocated for the duration
+ * of the call. Candidates: BFS alpha x beta; SSSP band sizes; batched BFS push fraction;
+ * SpGEMM register-tier limit x shared-table limit; TC task size x orientation. */
+apspie_status apspie_autotune(apspie_ctx *ctx, int32_t kind, const apspie_csr *A, const apspie_csr *B,
+                              const int32_t *sources, int32_t nsources, int32_t reps,
+                              apspie_tune_params *best, double *best_ms);
+/* The tuning table: entries, lookup of the set a call on A would use, and persistence as
+ * a text file (one entry per line; load merges, replacing entries of the same bucket). */
+int32_t apspie_tune_entries(const apspie_ctx *ctx);
+apspie_status apspie_tune_lookup(const apspie_ctx *ctx, int32_t kind, const apspie_csr *A,
+                                 apspie_tune_params *out, int32_t *found);
+apspie_status apspie_tune_save(const apspie_ctx *ctx, const char *path);
+apspie_status apspie_tune_load(apspie_ctx *ctx, const char *path);
+
 /* Checks a CSR on the device; APSPIE_OK or APSPIE_ERR_INVALID_ARG. */
 apspie_status apspie_csr_validate(apspie_ctx *ctx, const apspie_csr *A);
 
