@@ -96,6 +96,7 @@ struct apspie_ctx {
     int sssp_delta = 0;  // <= 0: chosen on the device
     long long sssp_band = 0;  // 0: auto, < 0: off
     int max_grid = 0;    // 0: as many co-resident blocks as fit
+    int grid_share = 1;  // persistent grids take 1/grid_share of the co-resident capacity
     float batch_push_frac = 0.05f;  // batched BFS: push while frontier edges < frac * nnz
     int spgemm_reg_max = 128;       // SpGEMM register tier: rows of <= this many products
     int spgemm_block_max = 1024;    // SpGEMM shared-table tier: rows of <= this many products

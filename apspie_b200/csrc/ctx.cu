@@ -4,6 +4,7 @@
 // per-call scratch (src/scratch.hpp:5-31, allocScratch src/util.cuh:646-672): the
 // reference mallocs scratch inside every call (and cub temp storage inside every level,
 // src/spmspvBfs.cuh:196-207); here one arena per context is grown on demand and reused.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -139,10 +140,13 @@ apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, vo
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, block, 0);
     if (e != cudaSuccess) return cuda_error(ctx, e, "occupancy query");
     if (per_sm < 1) return set_error(ctx, APSPIE_ERR_CUDA, "persistent kernel cannot be resident");
-    int grid = per_sm * ctx->num_sms;
+    // a context that shares the device with grid_share - 1 others takes 1/grid_share of
+    // the co-resident capacity, so that all of them fit at once
+    const int cap = std::max(1, per_sm * ctx->num_sms / std::max(1, ctx->grid_share));
+    int grid = cap;
     const long long want = (work + kWorkPerBlock - 1) / kWorkPerBlock;
     if (want < grid) grid = static_cast<int>(want < ctx->num_sms ? ctx->num_sms : want);
-    if (grid > per_sm * ctx->num_sms) grid = per_sm * ctx->num_sms;
+    if (grid > cap) grid = cap;
     if (ctx->max_grid > 0 && grid > ctx->max_grid) grid = ctx->max_grid;
     if (grid > kMaxGrid) grid = kMaxGrid;
     e = cudaLaunchCooperativeKernel(func, dim3(grid), dim3(block), args, 0, ctx->stream);

@@ -11,7 +11,10 @@
 //           into each request's output buffer;
 //   MIS  -> one apspie_mis (the fixed priorities make every MIS query on a graph the same
 //           question), the set copied to every waiting request;
-//   SSSP -> apspie_sssp_batch over up to max_batch sources, rows copied likewise.
+//   SSSP -> one apspie_sssp per request written straight into its output by default (the
+//           single-source kernel orders its work by distance band and beats the batched
+//           Bellman-Ford kernel per query), or, with apspie_server_set_sssp_fold(s, n > 1),
+//           apspie_sssp_batch over up to n sources, rows copied likewise.
 // A launch is admitted only if resident graphs + the slots' reserved scratch + the batch's
 // output staging fit the budget; otherwise it waits for a running launch to finish.
 // Requests that arrive while launches run are picked up by the next free slot (no wait for
@@ -78,6 +81,7 @@ struct apspie_server {
     int device = 0;
     int64_t budget = 0;
     int max_batch = 512;
+    int sssp_fold = 1;  // SSSP requests per launch (1: the single-source kernel)
     std::vector<apspie::Graph> graphs;
     size_t graph_bytes = 0;
     std::vector<apspie::Slot> slots;
@@ -101,12 +105,15 @@ namespace {
 // Scratch the launch reserves in the slot's arena, and batch output staging.
 size_t arena_need(const apspie_csr &g, int kind, int n) {
     if (kind == APSPIE_QUERY_BFS) return bfs_batch_scratch_need(g.m, n);
-    if (kind == APSPIE_QUERY_SSSP) return sssp_batch_scratch_need(g.m, n);
+    if (kind == APSPIE_QUERY_SSSP) return n == 1 ? traversal_scratch_need(g.m) : sssp_batch_scratch_need(g.m, n);
     return mis_scratch_need(g.m);
 }
 
+// Single SSSP requests write their answer directly; batches stage n rows.
+bool staged(int kind, int n) { return kind == APSPIE_QUERY_BFS || (kind == APSPIE_QUERY_SSSP && n > 1); }
+
 size_t stage_need(const apspie_csr &g, int kind, int n) {
-    return kind == APSPIE_QUERY_MIS ? 0 : static_cast<size_t>(n) * g.m * 4;
+    return staged(kind, n) ? static_cast<size_t>(n) * g.m * 4 : 0;
 }
 
 // Device bytes a slot holds now (its arena never shrinks; staging is kept for reuse).
@@ -122,7 +129,7 @@ size_t slot_growth(const Slot &sl, const apspie_csr &g, int kind, int n) {
     const size_t an = arena_need(g, kind, n);
     const size_t sn = stage_need(g, kind, n);
     return (an > cur ? an + an / 8 - cur : 0) + (sn > sl.stage_cap ? sn - sl.stage_cap : 0) +
-           (kind != APSPIE_QUERY_MIS && sl.src_cap < n ? static_cast<size_t>(std::max(n, 512)) * 4 : 0);
+           (staged(kind, n) && sl.src_cap < n ? static_cast<size_t>(std::max(n, 512)) * 4 : 0);
 }
 
 void finish_batch(apspie_server *s, Slot &sl) {
@@ -148,7 +155,10 @@ void launch_batch(apspie_server *s, Slot &sl) {
     const Graph &g = s->graphs[sl.batch.front().graph];
     apspie_status st = APSPIE_OK;
     const int n = static_cast<int>(sl.batch.size());
-    if (sl.kind == APSPIE_QUERY_BFS || sl.kind == APSPIE_QUERY_SSSP) {
+    if (sl.kind == APSPIE_QUERY_SSSP && n == 1) {
+        st = apspie_sssp(sl.ctx, &g.view, sl.batch.front().source, static_cast<int32_t *>(sl.batch.front().d_out),
+                         nullptr);
+    } else if (sl.kind == APSPIE_QUERY_BFS || sl.kind == APSPIE_QUERY_SSSP) {
         std::vector<int32_t> srcs(n);
         for (int i = 0; i < n; ++i) srcs[i] = sl.batch[i].source;
         const size_t rows = static_cast<size_t>(n) * g.view.m * sizeof(int32_t);
@@ -234,6 +244,7 @@ void worker_loop(apspie_server *s) {
             const Graph &g = s->graphs[gi];
             int n = static_cast<int>(best->second.size());
             if (kind != APSPIE_QUERY_MIS) n = std::min(n, s->max_batch);
+            if (kind == APSPIE_QUERY_SSSP) n = std::min(n, s->sssp_fold);
             size_t held = s->graph_bytes;
             for (auto &other : s->slots) held += slot_held(other);
             size_t need = slot_growth(sl, g.view, kind, n);
@@ -295,10 +306,12 @@ apspie_status apspie_server_create(int device, int64_t memory_budget_bytes, int3
             return APSPIE_ERR_CUDA;
         }
         sl.ctx->stream = sl.stream;
-        // Concurrent persistent grids must all fit on the device at once, or their grid
-        // barriers could wait on blocks that cannot be scheduled: with several slots each
-        // gets 2*SMs/slots blocks, under every traversal kernel's residency (>= 3 per SM).
-        if (num_slots > 1) apspie_ctx_set_max_grid(sl.ctx, std::max(1, 2 * sms / num_slots));
+        // Concurrent persistent grids should all fit on the device at once: each slot's
+        // grids take 1/num_slots of their kernel's co-resident capacity, so the slots'
+        // grids together use at most one device's worth of every SM resource. (A grid
+        // whose blocks could not all be resident would end its wait at a grid barrier with
+        // APSPIE_ERR_TIMEOUT, not hang.)
+        sl.ctx->grid_share = num_slots;
     }
     *out = s;
     return APSPIE_OK;
@@ -342,6 +355,12 @@ apspie_status apspie_server_add_graph(apspie_server *s, const apspie_host_csr *g
     s->slot_reserve = std::max(s->slot_reserve, traversal_scratch_need(G.view.m));
     s->graphs.push_back(G);
     *graph_id = static_cast<int32_t>(s->graphs.size() - 1);
+    return APSPIE_OK;
+}
+
+apspie_status apspie_server_set_sssp_fold(apspie_server *s, int32_t max_fold) {
+    if (!s || s->started || max_fold < 1) return APSPIE_ERR_INVALID_ARG;
+    s->sssp_fold = std::min(max_fold, s->max_batch);
     return APSPIE_OK;
 }
 

@@ -510,6 +510,9 @@ class Server:
         self.graphs.append(g)
         return gid.value
 
+    def set_sssp_fold(self, n: int) -> None:
+        L.check(L.lib().apspie_server_set_sssp_fold(self.handle, n), None, "server_set_sssp_fold")
+
     def start(self) -> None:
         L.check(L.lib().apspie_server_start(self.handle), None, "server_start")
 

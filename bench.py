@@ -405,7 +405,10 @@ def extras(ctx, args, ws, local):
                          "pull_levels": st["pull_iterations"]}
     del d20, o20, mem, prio
     res.update(extras_spgemm_tc(ctx, args, ws, local))
-    res.update(extras_batched(ctx, args, ws, local))
+    g22 = ap.gen_rmat(22, 16, 1, 3)  # weights for the serving leg; BFS ignores them
+    res.update(extras_batched(ctx, args, ws, local, g22))
+    if ws == 1:
+        res.update(extras_serving(ctx, args, local, g22))
     return res
 
 
@@ -451,7 +454,7 @@ def extras_spgemm_tc(ctx, args, ws, local):
     return res
 
 
-def extras_batched(ctx, args, ws, local):
+def extras_batched(ctx, args, ws, local, g):
     """Batched BFS on R-MAT scale 22 (seed 1): batches of 32/128/512 LCC sources (seed 6)
     against the plain path looping one source at a time over the same sources."""
     import torch
@@ -460,7 +463,6 @@ def extras_batched(ctx, args, ws, local):
     import oracle
 
     dev = f"cuda:{local}"
-    g = ap.gen_rmat(22, 16, 1, 3, weights=False)
     dg = ap.DeviceGraph(g, dev)
     srcs = ap.lcc_sample(g, 512, 6)
     one = torch.empty(g.m, dtype=torch.int32, device=dev)
@@ -481,6 +483,155 @@ def extras_batched(ctx, args, ws, local):
                                             "x_plain": plain_ms * nq / ms, "p99_ms": float(np.percentile(per, 99)),
                                             "exact_checked_rows": bool(exact)}
         del out
+    return res
+
+
+SERVE_QUERIES = 2000  # a bounded sample of the 100,000-query stream
+
+
+def serve_stream(graphs, n, rate_qps, seed=7):
+    """The request stream: from mt19937(seed) words, per query a kind (70 % BFS, 25 % SSSP,
+    5 % MIS), a graph (uniform), a source (uniform in that graph) and a Poisson arrival
+    (exponential gaps at rate_qps; rate 0 = all at t=0)."""
+    import apspie_b200 as ap
+
+    u = ap.mt19937_u32(seed, 4 * n).astype(np.float64).reshape(n, 4)
+    r = u[:, 0] % 100
+    kinds = np.where(r < 70, 0, np.where(r < 95, 1, 2)).astype(int)
+    which = (u[:, 1] % len(graphs)).astype(int)
+    srcs = [int(u[i, 2] % graphs[which[i]].m) for i in range(n)]
+    if rate_qps > 0:
+        gaps = -np.log1p(-u[:, 3] / 4294967296.0) / rate_qps
+        arrive = np.cumsum(gaps) - gaps[0]
+    else:
+        arrive = np.zeros(n)
+    return kinds, which, srcs, arrive
+
+
+def _pct(lat):
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p99.9_ms": float(np.percentile(lat, 99.9))}
+
+
+def serve_plain(ctx, dgs, prios, stream, dev):
+    """One query at a time through the plain entry points, FIFO in arrival order."""
+    import torch
+
+    kinds, which, srcs, arrive = stream
+    outs = [torch.empty(d.m, dtype=torch.int32, device=dev) for d in dgs]
+    mis_out = [torch.empty(d.m, dtype=torch.uint8, device=dev) for d in dgs]
+    lat = np.zeros(len(kinds))
+    t0 = time.perf_counter()
+    for i, (k, w, s) in enumerate(zip(kinds, which, srcs)):
+        now = time.perf_counter() - t0
+        if now < arrive[i]:
+            time.sleep(arrive[i] - now)
+        if k == 0:
+            ctx.bfs_into(dgs[w], s, outs[w])
+        elif k == 1:
+            ctx.sssp_into(dgs[w], s, outs[w])
+        else:
+            ctx.mis_into(dgs[w], prios[w], mis_out[w])
+        ctx.synchronize()
+        lat[i] = (time.perf_counter() - t0 - arrive[i]) * 1e3
+    total = time.perf_counter() - t0
+    return lat, total
+
+
+SERVE_SLOTS = 2  # measured best of 1, 2, 4, 8 on this mix
+
+
+def serve_server(graphs, stream, dev, check=(), slots=None):
+    """The same stream through apspie_server (4 slots, 40 GB budget); a waiter thread
+    collects completions while the main thread submits at the arrival times."""
+    import threading
+
+    import torch
+
+    import apspie_b200 as ap
+
+    kinds, which, srcs, arrive = stream
+    srv = ap.Server(int(dev.split(":")[1]), budget_bytes=40 << 30, slots=slots or SERVE_SLOTS, max_batch=512)
+    gids = [srv.add_graph(g) for g in graphs]
+    srv.start()
+    n = len(kinds)
+    tickets = [None] * n
+    outs = [None] * n
+    lat = np.zeros(n)
+    ready = threading.Semaphore(0)
+    keep = set(check)
+
+    def waiter():
+        for i in range(n):
+            ready.acquire()
+            lat[i] = srv.wait(tickets[i])
+            if i not in keep:
+                outs[i] = None
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    t0 = time.perf_counter()
+    for i in range(n):
+        now = time.perf_counter() - t0
+        if now < arrive[i]:
+            time.sleep(arrive[i] - now)
+        g = graphs[which[i]]
+        outs[i] = torch.empty(g.m, dtype=torch.uint8 if kinds[i] == 2 else torch.int32, device=dev)
+        tickets[i] = srv.submit(gids[which[i]], int(kinds[i]), srcs[i], outs[i])
+        ready.release()
+    th.join()
+    total = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    return lat, total, st, {i: outs[i] for i in keep}
+
+
+def extras_serving(ctx, args, local, g22):
+    """Serving on 4 resident R-MAT graphs (scales 16/18/20/22, edge factor 16, int32
+    weights [1,255]; seeds 16/18/2/1) under a 40 GB budget: a 2,000-query sample of the
+    70/25/5 BFS/SSSP/MIS stream, first all at once (saturation), then Poisson arrivals at
+    about 0.8x and 2x the plain path's saturated rate. The plain path runs the same
+    stream one query at a time, FIFO; a sample of server answers is checked against it."""
+    import torch
+
+    import apspie_b200 as ap
+
+    dev = f"cuda:{local}"
+    graphs = [ap.gen_rmat(16, 16, 16, 3), ap.gen_rmat(18, 16, 18, 3), ap.gen_rmat(20, 16, 2, 3), g22]
+    dgs = [ap.DeviceGraph(g, dev) for g in graphs]
+    prios = [torch.from_numpy(ap.mt19937_u32(4, g.m).view(np.int32)).to(dev) for g in graphs]
+    n = SERVE_QUERIES
+    sat = serve_stream(graphs, n, 0.0)
+    serve_plain(ctx, dgs, prios, serve_stream(graphs, 50, 0.0), dev)  # warm-up
+    lat_p, tot_p = serve_plain(ctx, dgs, prios, sat, dev)
+    plain_qps = n / tot_p
+    check = list(range(0, n, n // 40))
+    lat_s, tot_s, st, kept = serve_server(graphs, sat, dev, check)
+    exact = True
+    for i in check:
+        k, w, s = sat[0][i], sat[1][i], sat[2][i]
+        if k == 0:
+            ref = ctx.bfs(dgs[w], s)
+        elif k == 1:
+            ref = ctx.sssp(dgs[w], s)
+        else:
+            ref = ctx.mis(dgs[w], prios[w])
+        exact &= bool(torch.equal(ref, kept[i]))
+    res = {"serving": {
+        "workload": "4 graphs R-MAT s16/s18/s20/s22, 70/25/5 BFS/SSSP/MIS, 40 GB budget",
+        "slots": SERVE_SLOTS,
+        "queries": n, "plain_qps": plain_qps, "server_qps": n / tot_s, "x_plain": tot_p / tot_s,
+        "saturated": {"server": _pct(lat_s), "plain": _pct(lat_p)},
+        "launches": st["launches"], "max_batch_seen": st["max_batch_seen"], "peak_bytes": st["peak_bytes"],
+        "exact_checked": len(check), "exact": exact}}
+    for mult in (0.8, 2.0):
+        rate = mult * plain_qps
+        stream = serve_stream(graphs, n, rate)
+        lat_s, tot_s, _, _ = serve_server(graphs, stream, dev)
+        lat_p, tot_p = serve_plain(ctx, dgs, prios, stream, dev)
+        res["serving"][f"poisson_{mult}x_plain_rate"] = {
+            "rate_qps": rate, "server": dict(_pct(lat_s), qps=n / tot_s),
+            "plain": dict(_pct(lat_p), qps=n / tot_p)}
     return res
 
 

@@ -5,7 +5,8 @@
  * (test/bfs/run.sh, test/sssp/run.sh, test/mis/run.sh). The server keeps several graphs on
  * one GPU, admits BFS / SSSP / MIS requests against a device-memory budget and folds
  * requests that wait on the same graph into one launch (BFS: apspie_bfs_batch; SSSP:
- * apspie_sssp_batch; MIS: one apspie_mis shared by all waiting requests), on several
+ * one apspie_sssp per request, or apspie_sssp_batch when folding is enabled; MIS: one
+ * apspie_mis shared by all waiting requests), on several
  * execution slots whose launches overlap on the device. Each answer is written by the same
  * kernels as the plain entry points, so it is identical alone or in a mix.
  */
@@ -50,6 +51,10 @@ apspie_status apspie_server_create(int device, int64_t memory_budget_bytes, int3
  * undirected. MIS priorities are mt19937(mis_seed) outputs per vertex. Before start only. */
 apspie_status apspie_server_add_graph(apspie_server *s, const apspie_host_csr *g, int32_t symmetric,
                                       uint32_t mis_seed, int32_t *graph_id);
+/* SSSP requests folded into one launch (before start; default 1: each request runs the
+ * single-source kernel, which orders its work by distance band and is faster per query
+ * than the batched kernel on R-MAT graphs; n > 1 folds up to n into apspie_sssp_batch). */
+apspie_status apspie_server_set_sssp_fold(apspie_server *s, int32_t max_fold);
 /* Reserves the slots' scratch and starts the worker thread. */
 apspie_status apspie_server_start(apspie_server *s);
 /* Queues a request; the answer is written to d_out (device memory of the server's GPU),

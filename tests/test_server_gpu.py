@@ -32,9 +32,13 @@ def _out(g, kind):
     return torch.empty(g.m, dtype=torch.uint8 if kind == L.QUERY_MIS else torch.int32, device="cuda")
 
 
-def test_server_mix_matches_plain_path_alone_and_in_mix(ctx, graphs):
+@pytest.mark.parametrize("sssp_fold", [1, 64])
+def test_server_mix_matches_plain_path_alone_and_in_mix(ctx, graphs, sssp_fold):
+    """sssp_fold 1: each SSSP request runs the single-source kernel; 64: SSSP requests are
+    folded into the batched kernel like BFS requests."""
     srv = ap.Server(0, budget_bytes=8 << 30, slots=2, max_batch=512)
     gids = [srv.add_graph(g) for g in graphs]
+    srv.set_sssp_fold(sssp_fold)
     srv.start()
     rng = np.random.default_rng(7)
     kinds = rng.choice([L.QUERY_BFS, L.QUERY_SSSP, L.QUERY_MIS], size=400, p=[0.7, 0.25, 0.05])
