@@ -8,7 +8,8 @@
 // oldest pending request is oldest and folds every request of that pair that is waiting
 // at that moment into one launch:
 //   BFS  -> apspie_bfs_batch over up to max_batch sources, rows copied device-to-device
-//           into each request's output buffer;
+//           into each request's output buffer; fewer than bfs_min_batch waiting requests
+//           (6 by default) run apspie_bfs each instead, which is faster for so few;
 //   MIS  -> one apspie_mis (the fixed priorities make every MIS query on a graph the same
 //           question), the set copied to every waiting request;
 //   SSSP -> one apspie_sssp per request written straight into its output by default (the
@@ -82,6 +83,7 @@ struct apspie_server {
     int64_t budget = 0;
     int max_batch = 512;
     int sssp_fold = 1;  // SSSP requests per launch (1: the single-source kernel)
+    int bfs_min_batch = 6;  // fewer waiting BFS requests run the single-source kernel
     std::vector<apspie::Graph> graphs;
     size_t graph_bytes = 0;
     std::vector<apspie::Slot> slots;
@@ -102,18 +104,23 @@ struct apspie_server {
 namespace apspie {
 namespace {
 
-// Scratch the launch reserves in the slot's arena, and batch output staging.
-size_t arena_need(const apspie_csr &g, int kind, int n) {
-    if (kind == APSPIE_QUERY_BFS) return bfs_batch_scratch_need(g.m, n);
-    if (kind == APSPIE_QUERY_SSSP) return n == 1 ? traversal_scratch_need(g.m) : sssp_batch_scratch_need(g.m, n);
-    return mis_scratch_need(g.m);
+// A launch of n requests of `kind` runs the batched kernel when n reaches the kind's
+// minimum batch (BFS: bfs_min; SSSP: 2; MIS always folds); smaller launches run the
+// single-source kernel once per request, straight into each request's output.
+bool batched(int kind, int n, int bfs_min) {
+    return (kind == APSPIE_QUERY_BFS && n >= bfs_min) || (kind == APSPIE_QUERY_SSSP && n > 1);
 }
 
-// Single SSSP requests write their answer directly; batches stage n rows.
-bool staged(int kind, int n) { return kind == APSPIE_QUERY_BFS || (kind == APSPIE_QUERY_SSSP && n > 1); }
+// Scratch the launch reserves in the slot's arena.
+size_t arena_need(const apspie_csr &g, int kind, int n, int bfs_min) {
+    if (kind == APSPIE_QUERY_MIS) return mis_scratch_need(g.m);
+    if (!batched(kind, n, bfs_min)) return traversal_scratch_need(g.m);
+    return kind == APSPIE_QUERY_BFS ? bfs_batch_scratch_need(g.m, n) : sssp_batch_scratch_need(g.m, n);
+}
 
-size_t stage_need(const apspie_csr &g, int kind, int n) {
-    return staged(kind, n) ? static_cast<size_t>(n) * g.m * 4 : 0;
+// Batched launches stage their n rows before copying them out.
+size_t stage_need(const apspie_csr &g, int kind, int n, int bfs_min) {
+    return batched(kind, n, bfs_min) ? static_cast<size_t>(n) * g.m * 4 : 0;
 }
 
 // Device bytes a slot holds now (its arena never shrinks; staging is kept for reuse).
@@ -124,12 +131,12 @@ size_t slot_held(const Slot &sl) {
 
 // Extra device bytes running (kind, n) on the slot would allocate (arena growth keeps
 // 1/8 headroom, as scratch_reserve does).
-size_t slot_growth(const Slot &sl, const apspie_csr &g, int kind, int n) {
+size_t slot_growth(const Slot &sl, const apspie_csr &g, int kind, int n, int bfs_min) {
     const size_t cur = static_cast<size_t>(apspie_ctx_scratch_bytes(sl.ctx));
-    const size_t an = arena_need(g, kind, n);
-    const size_t sn = stage_need(g, kind, n);
+    const size_t an = arena_need(g, kind, n, bfs_min);
+    const size_t sn = stage_need(g, kind, n, bfs_min);
     return (an > cur ? an + an / 8 - cur : 0) + (sn > sl.stage_cap ? sn - sl.stage_cap : 0) +
-           (staged(kind, n) && sl.src_cap < n ? static_cast<size_t>(std::max(n, 512)) * 4 : 0);
+           (batched(kind, n, bfs_min) && sl.src_cap < n ? static_cast<size_t>(std::max(n, 512)) * 4 : 0);
 }
 
 void finish_batch(apspie_server *s, Slot &sl) {
@@ -155,9 +162,13 @@ void launch_batch(apspie_server *s, Slot &sl) {
     const Graph &g = s->graphs[sl.batch.front().graph];
     apspie_status st = APSPIE_OK;
     const int n = static_cast<int>(sl.batch.size());
-    if (sl.kind == APSPIE_QUERY_SSSP && n == 1) {
-        st = apspie_sssp(sl.ctx, &g.view, sl.batch.front().source, static_cast<int32_t *>(sl.batch.front().d_out),
-                         nullptr);
+    if (sl.kind != APSPIE_QUERY_MIS && !batched(sl.kind, n, s->bfs_min_batch)) {
+        for (int i = 0; i < n && st == APSPIE_OK; ++i) {
+            const Request &r = sl.batch[i];
+            st = sl.kind == APSPIE_QUERY_BFS
+                     ? apspie_bfs(sl.ctx, &g.view, r.source, 0, static_cast<int32_t *>(r.d_out), nullptr)
+                     : apspie_sssp(sl.ctx, &g.view, r.source, static_cast<int32_t *>(r.d_out), nullptr);
+        }
     } else if (sl.kind == APSPIE_QUERY_BFS || sl.kind == APSPIE_QUERY_SSSP) {
         std::vector<int32_t> srcs(n);
         for (int i = 0; i < n; ++i) srcs[i] = sl.batch[i].source;
@@ -247,11 +258,11 @@ void worker_loop(apspie_server *s) {
             if (kind == APSPIE_QUERY_SSSP) n = std::min(n, s->sssp_fold);
             size_t held = s->graph_bytes;
             for (auto &other : s->slots) held += slot_held(other);
-            size_t need = slot_growth(sl, g.view, kind, n);
+            size_t need = slot_growth(sl, g.view, kind, n, s->bfs_min_batch);
             // shrink the batch until its growth fits the budget
             while (n > 1 && held + need > static_cast<size_t>(s->budget)) {
                 n /= 2;
-                need = slot_growth(sl, g.view, kind, n);
+                need = slot_growth(sl, g.view, kind, n, s->bfs_min_batch);
             }
             const size_t fixed = held;
             if (held + need > static_cast<size_t>(s->budget)) {
@@ -361,6 +372,12 @@ apspie_status apspie_server_add_graph(apspie_server *s, const apspie_host_csr *g
 apspie_status apspie_server_set_sssp_fold(apspie_server *s, int32_t max_fold) {
     if (!s || s->started || max_fold < 1) return APSPIE_ERR_INVALID_ARG;
     s->sssp_fold = std::min(max_fold, s->max_batch);
+    return APSPIE_OK;
+}
+
+apspie_status apspie_server_set_bfs_min_batch(apspie_server *s, int32_t min_batch) {
+    if (!s || s->started || min_batch < 1) return APSPIE_ERR_INVALID_ARG;
+    s->bfs_min_batch = min_batch;
     return APSPIE_OK;
 }
 

@@ -510,6 +510,9 @@ class Server:
         self.graphs.append(g)
         return gid.value
 
+    def set_bfs_min_batch(self, n: int) -> None:
+        L.check(L.lib().apspie_server_set_bfs_min_batch(self.handle, n), None, "server_set_bfs_min_batch")
+
     def set_sssp_fold(self, n: int) -> None:
         L.check(L.lib().apspie_server_set_sssp_fold(self.handle, n), None, "server_set_sssp_fold")
 

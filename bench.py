@@ -626,6 +626,15 @@ def extras_serving(ctx, args, local, g22):
         "saturated": {"server": _pct(lat_s), "plain": _pct(lat_p)},
         "launches": st["launches"], "max_batch_seen": st["max_batch_seen"], "peak_bytes": st["peak_bytes"],
         "exact_checked": len(check), "exact": exact}}
+    # BFS-only stream on the scale-22 graph: the batched-serving target
+    bstream = serve_stream(graphs, n, 0.0)
+    bstream = (np.zeros(n, dtype=int), np.full(n, 3), bstream[2], bstream[3])
+    bstream = (bstream[0], bstream[1], [int(x) % graphs[3].m for x in bstream[2]], bstream[3])
+    lat_p, tot_p = serve_plain(ctx, dgs, prios, bstream, dev)
+    lat_s, tot_s, st, _ = serve_server(graphs, bstream, dev)
+    res["serving"]["bfs_only_rmat22_saturated"] = {
+        "plain_qps": n / tot_p, "server_qps": n / tot_s, "x_plain": tot_p / tot_s, "server": _pct(lat_s),
+        "plain": _pct(lat_p), "launches": st["launches"], "max_batch_seen": st["max_batch_seen"]}
     for mult in (0.8, 2.0):
         rate = mult * plain_qps
         stream = serve_stream(graphs, n, rate)

@@ -55,6 +55,9 @@ apspie_status apspie_server_add_graph(apspie_server *s, const apspie_host_csr *g
  * single-source kernel, which orders its work by distance band and is faster per query
  * than the batched kernel on R-MAT graphs; n > 1 folds up to n into apspie_sssp_batch). */
 apspie_status apspie_server_set_sssp_fold(apspie_server *s, int32_t max_fold);
+/* BFS requests run the batched kernel only when at least min_batch of them wait on the
+ * same graph (before start; default 6); fewer run apspie_bfs each. */
+apspie_status apspie_server_set_bfs_min_batch(apspie_server *s, int32_t min_batch);
 /* Reserves the slots' scratch and starts the worker thread. */
 apspie_status apspie_server_start(apspie_server *s);
 /* Queues a request; the answer is written to d_out (device memory of the server's GPU),
