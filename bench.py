@@ -627,9 +627,8 @@ def extras_serving(ctx, args, local, g22):
         "launches": st["launches"], "max_batch_seen": st["max_batch_seen"], "peak_bytes": st["peak_bytes"],
         "exact_checked": len(check), "exact": exact}}
     # BFS-only stream on the scale-22 graph: the batched-serving target
-    bstream = serve_stream(graphs, n, 0.0)
-    bstream = (np.zeros(n, dtype=int), np.full(n, 3), bstream[2], bstream[3])
-    bstream = (bstream[0], bstream[1], [int(x) % graphs[3].m for x in bstream[2]], bstream[3])
+    words = ap.mt19937_u32(8, n).astype(np.int64)
+    bstream = (np.zeros(n, dtype=int), np.full(n, 3), [int(w % graphs[3].m) for w in words], np.zeros(n))
     lat_p, tot_p = serve_plain(ctx, dgs, prios, bstream, dev)
     lat_s, tot_s, st, _ = serve_server(graphs, bstream, dev)
     res["serving"]["bfs_only_rmat22_saturated"] = {
