@@ -158,13 +158,15 @@ struct RegTierSmem {
     V av[N];          // A values
     V pv[N];          // product values, by product index
     unsigned skey[N]; // sorted keys (numeric: walked by the head of each run)
+    int tab[2 * N];   // symbolic: hash set of the row's columns
 };
 
 // One warp per row of at most N = 32 * PL products. Product q (element r * 32 + lane) of
 // A entry t gets the key (column << QB) | q; after a bitonic sort of the keys in registers
 // the products of one output column are adjacent and in increasing q, i.e. increasing
 // position in A's row, so a run's head sums them in the oracle's order (bit-identical
-// FP32). Requires B->n <= 2^24 (see bin_of).
+// FP32). The symbolic pass only counts distinct columns, with a 2N-slot shared-memory hash
+// set instead of the sort. Requires B->n <= 2^24 (see bin_of).
 template <int PL, bool NUMERIC, typename V>
 __global__ void __launch_bounds__(kSgBlock) sg_reg(const int *__restrict__ rows, int nrows, Mat A, Mat B,
                                                    int *cnt, const int *__restrict__ crp, int *cci, V *cval) {
@@ -234,6 +236,33 @@ __global__ void __launch_bounds__(kSgBlock) sg_reg(const int *__restrict__ rows,
                 if (NUMERIC) sm.pv[q] = vmul<V>(sm.av[lo], bval[e]);
             }
         }
+        if (!NUMERIC) {
+            // count distinct columns: insert into the (half-full at most) set
+#pragma unroll
+            for (int r = 0; r < 2 * PL; ++r) sm.tab[r * 32 + lane] = -1;
+            __syncwarp();
+            int fresh = 0;
+#pragma unroll
+            for (int r = 0; r < PL; ++r) {
+                if (key[r] == PAD) continue;
+                const int col = static_cast<int>(key[r] >> QB);
+                unsigned slot = (static_cast<unsigned>(col) * 2654435761u) >> (32 - (QB + 1));
+                for (int probe = 0; probe < 2 * N; ++probe) {
+                    const int old = atomicCAS(&sm.tab[slot], -1, col);
+                    if (old == -1) {
+                        ++fresh;
+                        break;
+                    }
+                    if (old == col) break;
+                    slot = (slot + 1) & (2 * N - 1);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) fresh += __shfl_down_sync(0xffffffffu, fresh, o);
+            if (lane == 0) cnt[i] = fresh;
+            __syncwarp();
+            continue;
+        }
         // bitonic sort of the N keys, element index r * 32 + lane
 #pragma unroll
         for (int k = 2; k <= N; k <<= 1) {
@@ -266,7 +295,6 @@ __global__ void __launch_bounds__(kSgBlock) sg_reg(const int *__restrict__ rows,
         // run heads: first element of each column
         bool head[PL];
         unsigned hmask[PL];
-        int count = 0;
 #pragma unroll
         for (int r = 0; r < PL; ++r) {
             unsigned prev = __shfl_up_sync(0xffffffffu, key[r], 1);
@@ -276,11 +304,6 @@ __global__ void __launch_bounds__(kSgBlock) sg_reg(const int *__restrict__ rows,
             }
             head[r] = key[r] != PAD && ((r == 0 && lane == 0) || (prev >> QB) != (key[r] >> QB));
             hmask[r] = __ballot_sync(0xffffffffu, head[r]);
-            count += __popc(hmask[r]);
-        }
-        if (!NUMERIC) {
-            if (lane == 0) cnt[i] = count;
-            continue;
         }
 #pragma unroll
         for (int r = 0; r < PL; ++r) sm.skey[r * 32 + lane] = key[r];

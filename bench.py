@@ -242,6 +242,19 @@ def main_ours(args, ws, rank, local):
 
     torch.cuda.set_device(local)
     dev = f"cuda:{local}"
+    if args.only_extra:
+        # one extra leg alone (for profiling a kernel without the rest of the run)
+        ctx = ap.Context(local)
+        if args.only_extra == "spgemm_tc":
+            res = extras_spgemm_tc(ctx, args, ws, local)
+        else:
+            g22 = ap.gen_rmat(22, 16, 1, 3)
+            res = extras_batched(ctx, args, ws, local, g22) if args.only_extra == "batched" \
+                else extras_serving(ctx, args, local, g22)
+        ctx.close()
+        if rank == 0:
+            print(json.dumps({"extra": res}))
+        return 0
     g, src = build_graph(20, 2)
     ctx = ap.Context(local)
     stream = ctx.stream
@@ -653,6 +666,8 @@ def main():
     ap_.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap_.add_argument("--no-extra", action="store_true")
     ap_.add_argument("--no-cpu-baseline", action="store_true")
+    ap_.add_argument("--only-extra", choices=["spgemm_tc", "batched", "serving"], default=None,
+                     help="run one extra leg alone and print its JSON (no headline line)")
     args = ap_.parse_args()
     ws, rank, local = dist_env()
     if ws > 1 and args.impl == "ours":
