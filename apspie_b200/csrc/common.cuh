@@ -204,9 +204,9 @@ __device__ __forceinline__ void raise_error(TravCtl *ctl, int *sticky, int statu
     atomicCAS(sticky, 0, status);
 }
 
-__device__ __forceinline__ unsigned long long ld_volatile_u64(const void *p) {
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const void *p) {
     unsigned long long v;
-    asm volatile("ld.volatile.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -228,7 +228,7 @@ __device__ __forceinline__ bool grid_barrier(TravCtl *ctl, int *sticky, int wher
         unsigned long long pair;
         unsigned long long t0 = 0;
         for (unsigned spin = 1;; ++spin) {
-            pair = ld_volatile_u64(&ctl->bar);
+            pair = ld_acquire_u64(&ctl->bar);
             if (((static_cast<unsigned>(pair) ^ before) & 0x80000000u) != 0u) break;
             if ((pair >> 32) != 0ull) break;  // an error was raised: leave now
             if ((spin & 1023u) == 0u) {

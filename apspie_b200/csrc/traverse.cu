@@ -504,11 +504,19 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
                 int ndef = 0;
 #pragma unroll
                 for (int k = 0; k < PA; ++k) {
-                    if (defer[k]) {
-                        atomicAdd(&sh.hist[band_bin(d[k], base_i, is_float_a, inv_unit)],
-                                  static_cast<unsigned long long>(r1[k] - r0[k]));
-                        atomicMin(&sh.hmin, d[k]);
+                    // deferred entries of a warp mostly share one bin: one atomic then
+                    const int bin = defer[k] ? band_bin(d[k], base_i, is_float_a, inv_unit) : -1;
+                    const int bin0 = __shfl_sync(0xffffffffu, bin, 0);
+                    if (__all_sync(0xffffffffu, bin == bin0)) {
+                        const unsigned tot =
+                            __reduce_add_sync(0xffffffffu, static_cast<unsigned>(min(r1[k] - r0[k], 1 << 26)));
+                        if (bin0 >= 0 && (threadIdx.x & 31) == 0)
+                            atomicAdd(&sh.hist[bin0], static_cast<unsigned long long>(tot));
+                    } else if (defer[k]) {
+                        atomicAdd(&sh.hist[bin], static_cast<unsigned long long>(r1[k] - r0[k]));
                     }
+                    const int mn = __reduce_min_sync(0xffffffffu, defer[k] ? d[k] : 0x7fffffff);
+                    if (mn != 0x7fffffff && (threadIdx.x & 31) == 0) atomicMin(&sh.hmin, mn);
                     ndef += defer[k] ? 1 : 0;
                 }
                 // one scan carries both the edge count (high half) and the deferred count
