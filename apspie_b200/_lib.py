@@ -107,6 +107,7 @@ SIGNATURES = {
     "apspie_ctx_set_bfs_tuning": (c_int, [c_void_p, c_float, c_float]),
     "apspie_ctx_set_sssp_delta": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_set_sssp_band": (c_int, [c_void_p, c_int64]),
+    "apspie_ctx_set_sssp_batch_groups": (c_int, [c_void_p, c_int32]),
     "apspie_ctx_get_params": (c_int, [c_void_p, POINTER(TuneParams)]),
     "apspie_ctx_set_params": (c_int, [c_void_p, POINTER(TuneParams)]),
     "apspie_ctx_set_autotune": (c_int, [c_void_p, c_int32]),

@@ -102,6 +102,7 @@ struct apspie_ctx {
     int spgemm_block_max = 1024;    // SpGEMM shared-table tier: rows of <= this many products
     int tc_task_work = 4096;        // TC wedges per warp task
     int tc_orient = 1;              // TC: re-orient L by degree
+    int sssp_batch_groups = 0;      // batched SSSP: 0 auto, > 0 query groups, < 0 multi-query kernel
     int use_tuning = 1;             // consult tune_table
     std::vector<apspie_tune_entry> tune_table;
 };
@@ -137,6 +138,11 @@ size_t traversal_scratch_need(int m);        // apspie_bfs / apspie_sssp
 size_t mis_scratch_need(int m);              // apspie_mis
 size_t bfs_batch_scratch_need(int m, int nq);  // apspie_bfs_batch (nq <= 512 per launch)
 size_t sssp_batch_scratch_need(int m, int nq);  // apspie_sssp_batch (nq <= 512 per launch)
+// apspie_sssp_batch in query groups (each group of blocks runs single-source SSSPs)
+size_t sssp_group_scratch_need(int m, int groups);
+int sssp_group_count(const apspie_ctx *ctx, int nq);
+apspie_status sssp_batch_grouped(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources, int32_t nq,
+                                 int32_t *d_dists, apspie_run_stats *stats);
 
 // Device-wide exclusive scan (scan.cu): out[0..n) = prefix of in, out[n] = total.
 size_t scan_scratch_bytes(long long n);
@@ -210,6 +216,15 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const void *p) {
     return v;
 }
 
+// The blocks that cooperate on one traversal: all of a launch's blocks, or one group of
+// them when a launch runs several independent traversals side by side.
+struct VGrid {
+    int id;  // this block's index within the group
+    int n;   // blocks in the group
+};
+
+__device__ __forceinline__ VGrid hw_grid() { return VGrid{static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x)}; }
+
 // Grid-wide barrier for a cooperatively launched (co-resident) grid: a sense-reversing
 // counter. Thread 0 of every block adds 1 to ctl->bar, except block 0, which adds
 // 2^31 - (G - 1); the G additions sum to 2^31, so bit 31 flips exactly when the last block
@@ -218,11 +233,12 @@ __device__ __forceinline__ unsigned long long ld_acquire_u64(const void *p) {
 // or until an error is posted. Every wait is bounded by kBarrierTimeoutNs; on timeout it
 // raises APSPIE_ERR_TIMEOUT. Returns false when any block has raised an error, so that all
 // blocks leave the persistent loop together instead of hanging.
-__device__ __forceinline__ bool grid_barrier(TravCtl *ctl, int *sticky, int where) {
+// With a VGrid group, the group's blocks synchronise on the group's own control block.
+__device__ __forceinline__ bool grid_barrier(TravCtl *ctl, int *sticky, int where, VGrid vg = hw_grid()) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1) : 1u;
+        const unsigned inc = vg.id == 0 ? 0x80000000u - static_cast<unsigned>(vg.n - 1) : 1u;
         __threadfence();
         const unsigned before = atomicAdd(&ctl->bar, inc);
         unsigned long long pair;

@@ -278,6 +278,12 @@ apspie_status apspie_ctx_set_sssp_band(apspie_ctx *ctx, int64_t edges) {
     return APSPIE_OK;
 }
 
+apspie_status apspie_ctx_set_sssp_batch_groups(apspie_ctx *ctx, int32_t groups) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    ctx->sssp_batch_groups = groups;
+    return APSPIE_OK;
+}
+
 apspie_status apspie_ctx_set_batch_push_frac(apspie_ctx *ctx, float frac) {
     if (!ctx || !(frac >= 0.0f)) return APSPIE_ERR_INVALID_ARG;
     ctx->batch_push_frac = frac;

@@ -70,10 +70,10 @@ template <int BLOCK, class Hook, class RowOf = RowIsEntry>
 __device__ __forceinline__ void frontier_phase_a(const int *__restrict__ q, int nf,
                                                  const int *__restrict__ row_ptr, int *rs,
                                                  int *loc_off, int *chunk_sum, int *scan_tmp,
-                                                 Hook hook, RowOf row_of = RowOf()) {
-    const int G = gridDim.x;
+                                                 Hook hook, RowOf row_of = RowOf(), VGrid vg = hw_grid()) {
+    const int G = vg.n;
     const int C = (nf + G - 1) / G;
-    const int c0 = min(static_cast<int>(blockIdx.x) * C, nf);
+    const int c0 = min(vg.id * C, nf);
     const int c1 = min(c0 + C, nf);
     int carry = 0;
     for (int base = c0; base < c1; base += BLOCK) {
@@ -92,15 +92,15 @@ __device__ __forceinline__ void frontier_phase_a(const int *__restrict__ q, int 
         if (i < c1) loc_off[i] = carry + ex;
         carry += tot;
     }
-    if (threadIdx.x == 0) chunk_sum[blockIdx.x] = carry;
+    if (threadIdx.x == 0) chunk_sum[vg.id] = carry;
 }
 
 // Loads the chunk totals of phase A into base[] as an exclusive prefix; returns the total
 // number of edges of the frontier.
 template <int BLOCK>
 __device__ __forceinline__ int frontier_chunk_bases(const int *__restrict__ chunk_sum, int *base,
-                                                    int *scan_tmp) {
-    const int G = gridDim.x;
+                                                    int *scan_tmp, VGrid vg = hw_grid()) {
+    const int G = vg.n;
     const int per = (G + BLOCK - 1) / BLOCK;
     const int t0 = threadIdx.x * per;
     int local = 0;
@@ -160,17 +160,17 @@ template <int BLOCK, int VT, bool EXTRA, class Load, class Op, class Post>
 __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__restrict__ loc_off,
                                                 const int *__restrict__ rs,
                                                 ExpandSmem<BLOCK, VT, EXTRA> &sm, Load load, Op op,
-                                                Post post) {
+                                                Post post, VGrid vg = hw_grid()) {
     using S = ExpandSmem<BLOCK, VT, EXTRA>;
     constexpr int WT = S::WT;
     constexpr int NWARP = S::NWARP;
     constexpr int BATCH = S::BATCH;
-    const int G = gridDim.x;
+    const int G = vg.n;
     const int C = (nf + G - 1) / G;
     const long long total = static_cast<long long>(nf) + E;
     const long long ntiles = (total + WT - 1) / WT;
     const long long per = (ntiles + G - 1) / G;
-    const long long t_begin = static_cast<long long>(blockIdx.x) * per;
+    const long long t_begin = static_cast<long long>(vg.id) * per;
     const long long t_end = t_begin + per < ntiles ? t_begin + per : ntiles;
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;

@@ -1,5 +1,10 @@
 // Batched multi-source SSSP: many sources on one resident graph in ONE persistent launch.
 //
+// By default apspie_sssp_batch runs the query groups of traverse.cu (each group of blocks
+// runs the banded single-source SSSP on its share of the sources). The multi-query kernel
+// below (apspie_ctx_set_sssp_batch_groups(ctx, -1)) reads each frontier row once for
+// all of its queries instead, but relaxes in Bellman-Ford order.
+//
 // Frontier entries are (vertex u, query word w) pairs whose "changed" bits (the queries
 // whose distance at u dropped in the previous iteration) are non-zero; an entry's weight
 // is deg(u), so the merge-path expander balances the edges, and every lane relaxes its
@@ -183,7 +188,10 @@ __global__ void __launch_bounds__(kSbBlock) sssp_batch_kernel(SbArgs a) {
 size_t sssp_batch_scratch_need(int m, int nq) {
     const int W = ((nq < 512 ? nq : 512) + 31) / 32;
     const size_t mw = static_cast<size_t>(m) * (W > 0 ? W : 1);
-    return Carver::need({mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, kMaxGrid * 4});
+    const size_t multi = Carver::need({mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, kMaxGrid * 4});
+    // the default grouped form: up to 4 groups
+    const size_t grouped = sssp_group_scratch_need(m, std::max(1, std::min(nq, 4)));
+    return std::max(multi, grouped);
 }
 
 }  // namespace apspie
@@ -203,6 +211,7 @@ extern "C" apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A,
     if (num_sources < 0 || (num_sources > 0 && (!d_sources || !d_dists)))
         return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp_batch: bad sources/output");
     if (ctx->validate && (st = validate_csr(ctx, A, true)) != APSPIE_OK) return st;
+    if (ctx->sssp_batch_groups >= 0) return sssp_batch_grouped(ctx, A, d_sources, num_sources, d_dists, stats);
     const int m = A->m;
     // queries per launch: W words with (nnz + m) * W below 2^31 (int32 item counts)
     long long wmax = 0x7fffffffLL / (static_cast<long long>(A->nnz) + m + 1);

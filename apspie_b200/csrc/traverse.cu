@@ -59,6 +59,7 @@ enum : int {
     kSiteSsspBarB = 211,
     kSiteSsspBarF0 = 212,
     kSiteSsspBarF1 = 213,
+    kSiteSsspGroup = 214,  // and 215
     kSiteMis = 300,
     kSiteMisRoundCap = 301,
 };
@@ -316,13 +317,13 @@ struct SsspShared {
 // stops after the CPU BFS depth; here a relaxation is a plain read of dist[v] and, only
 // if it improves, an atomicMin, and the loop ends when both piles are empty. The result is
 // the exact fixed point for non-negative integer weights, independent of relaxation order.
-__global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs a) {
+__device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
     static_assert(kBlock == kBandBins, "one histogram bin per thread");
     __shared__ SsspShared sh;
     SsspSmem &sm = sh.ex;
     timeline_mark(a.ctl, 0);
-    const int G = gridDim.x;
-    const int gtid = blockIdx.x * kBlock + threadIdx.x;
+    const int G = vg.n;
+    const int gtid = vg.id * kBlock + threadIdx.x;
     const int gstride = G * kBlock;
     const int m = a.m;
     const int words = (m + 31) >> 5;
@@ -364,7 +365,7 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
     }
     sh.hist[threadIdx.x] = 0ull;
     if (threadIdx.x == 0) sh.hmin = INF;
-    if (!grid_barrier(a.ctl, a.sticky, kSiteSssp)) return;
+    if (!grid_barrier(a.ctl, a.sticky, kSiteSssp, vg)) return;
 
     const bool banded = a.band > 0;
     const double sum_w = __longlong_as_double(__ldcg(&a.ctl->aux[0]));
@@ -403,10 +404,10 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
             if (nfar == 0) break;
             thresh += delta;
             // every block must have read qlen[cur] (== 0) before any block appends to it
-            if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarF0)) return;
+            if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarF0, vg)) return;
             WQ wn(sm.qbuf[threadIdx.x >> 5][0], qc, &a.ctl->qlen[cur]);
             WQ wf(sm.qbuf[threadIdx.x >> 5][1], fnext, &a.ctl->flen[fc ^ 1]);
-            for (int base = blockIdx.x * kBlock; base < nfar; base += gstride) {
+            for (int base = vg.id * kBlock; base < nfar; base += gstride) {
                 const int i = base + threadIdx.x;
                 bool to_near = false, stay = false;
                 int v = 0;
@@ -428,7 +429,7 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
             }
             wn.flush();
             wf.flush();
-            if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarF1)) return;
+            if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarF1, vg)) return;
             if (gtid == 0) a.ctl->flen[fc] = 0;  // drained; every block read nfar above
             fc ^= 1;
             continue;
@@ -459,7 +460,7 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
             // layout (chunk c = entries [c*C, (c+1)*C)) is the one frontier_expand reads
             constexpr int PA = kSsspPA;
             const int C = (nf + G - 1) / G;
-            const int c0 = min(static_cast<int>(blockIdx.x) * C, nf);
+            const int c0 = min(vg.id * C, nf);
             const int c1 = min(c0 + C, nf);
             const int *rpa = a.row_ptr;
             int carry = 0;
@@ -540,9 +541,9 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
                 carry += static_cast<int>(total >> 32);
                 __syncthreads();  // sh.scan and sh.dbase are reused by the next step
             }
-            if (threadIdx.x == 0) a.buf.chunk_sum[blockIdx.x] = carry;
+            if (threadIdx.x == 0) a.buf.chunk_sum[vg.id] = carry;
         }
-        if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarA)) return;
+        if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarA, vg)) return;
         // every block has read this queue's length, base and histogram: reset them for the
         // iteration that fills this queue next
         if (gtid < kBandBins) a.ctl->shist[cur][gtid] = 0ull;
@@ -551,7 +552,7 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
             a.ctl->sbase[cur] = INF;
         }
 
-        const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
+        const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp, vg);
         expanded += E;
         ++iters;
         const int *col = a.col_ind;
@@ -649,7 +650,7 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
                     wf.push(far[r], v[r]);
                 }
             },
-            NoPost());
+            NoPost(), vg);
         wn.flush();
         wf.flush();
         if (banded) {
@@ -664,7 +665,7 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
                 sh.hmin = INF;
             }
         }
-        if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarB)) return;
+        if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarB, vg)) return;
         cur ^= 1;
     }
     // unreached -> -1, and the component statistics
@@ -695,6 +696,75 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs
         a.ctl->edges_expanded = expanded;
         a.ctl->delta = delta < 2147483647.0 ? static_cast<int>(delta) : 0;  // 0: no far pile
     }
+}
+
+__global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_kernel(SsspArgs a) { sssp_body(a, hw_grid()); }
+
+// Many sources in one launch: the grid splits into `groups` equal groups of blocks, each
+// with its own control block and scratch, and each group runs the single-source SSSP
+// above on queries grp, grp + groups, ... in turn, synchronising only among its own
+// blocks. Every answer is the single-source kernel's answer; the queries of different
+// groups run side by side, which pays because one query alone keeps the device
+// latency-bound (few warps issue at a time).
+struct SsspGroupArgs {
+    SsspArgs base;       // graph, weights, band, sticky word; per query: src, dist, ctl, buf
+    const int *srcs;
+    int *out;            // nq x m, query-major
+    int nq, groups, m;
+    TravCtl *ctls;       // one control block per group
+    size_t buf_stride;   // bytes between consecutive groups' scratch (base.buf is group 0's)
+    TravCtl *main;       // the context's control block: errors and summed statistics
+};
+
+__device__ __forceinline__ TravBuffers shift_buffers(TravBuffers b, size_t off) {
+    auto sh = [off](auto *p) { return reinterpret_cast<decltype(p)>(reinterpret_cast<char *>(p) + off); };
+    b.q0 = sh(b.q0);
+    b.q1 = sh(b.q1);
+    b.q2 = sh(b.q2);
+    b.q3 = sh(b.q3);
+    b.rs = sh(b.rs);
+    b.loc_off = sh(b.loc_off);
+    b.chunk_sum = sh(b.chunk_sum);
+    b.aux = sh(b.aux);
+    b.aux2 = sh(b.aux2);
+    b.bits0 = sh(b.bits0);
+    b.bits1 = sh(b.bits1);
+    b.bits2 = sh(b.bits2);
+    return b;
+}
+
+__global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_group_kernel(SsspGroupArgs g) {
+    const int bpg = static_cast<int>(gridDim.x) / g.groups;  // the host launches groups * bpg blocks
+    const int grp = static_cast<int>(blockIdx.x) / bpg;
+    const VGrid vg{static_cast<int>(blockIdx.x) - grp * bpg, bpg};
+    TravCtl *ctl = g.ctls + grp;
+    SsspArgs a = g.base;
+    a.ctl = ctl;
+    a.buf = shift_buffers(g.base.buf, g.buf_stride * grp);
+    const int tid = vg.id * kBlock + static_cast<int>(threadIdx.x);
+    for (int q = grp; q < g.nq; q += g.groups) {
+        a.src = __ldg(g.srcs + q);
+        a.dist = g.out + static_cast<size_t>(q) * g.m;
+        sssp_body(a, vg);
+        // every block of the group is done with the control block before it is reset
+        if (!grid_barrier(ctl, a.sticky, kSiteSsspGroup, vg)) break;
+        if (tid == 0) {
+            atomicAdd(reinterpret_cast<unsigned long long *>(&g.main->edges_expanded),
+                      static_cast<unsigned long long>(ctl->edges_expanded));
+            atomicAdd(reinterpret_cast<unsigned long long *>(&g.main->edges_component),
+                      static_cast<unsigned long long>(ctl->edges_component));
+            atomicAdd(reinterpret_cast<unsigned long long *>(&g.main->vertices_reached),
+                      static_cast<unsigned long long>(ctl->vertices_reached));
+            atomicAdd(&g.main->iterations, ctl->iterations);
+            atomicAdd(&g.main->push_iterations, ctl->push_iterations);
+            ctl->edges_component = 0;
+            ctl->vertices_reached = 0;
+            for (int k = 0; k < 4; ++k) ctl->aux[k] = 0;
+        }
+        for (int k = tid; k < 2 * kBandBins; k += vg.n * kBlock) ctl->shist[k / kBandBins][k % kBandBins] = 0ull;
+        if (!grid_barrier(ctl, a.sticky, kSiteSsspGroup + 1, vg)) break;
+    }
+    if (tid == 0 && ctl->err != 0) raise_error(g.main, a.sticky, ctl->err, ctl->err_where);
 }
 
 // ================================================================================
@@ -1063,6 +1133,77 @@ apspie_status sssp_common(apspie_ctx *ctx, const apspie_csr *A, int32_t source, 
     return finish_call(ctx, stats, "apspie_sssp");
 }
 }  // namespace
+
+size_t sssp_group_scratch_need(int m, int groups) {
+    const size_t per = (trav_scratch_bytes(m) + 255) / 256 * 256;
+    return per * static_cast<size_t>(groups) + static_cast<size_t>(groups) * ((sizeof(TravCtl) + 255) / 256 * 256);
+}
+
+int sssp_group_count(const apspie_ctx *ctx, int nq) {
+    int g = ctx->sssp_batch_groups > 0 ? ctx->sssp_batch_groups : 4;
+    return std::max(1, std::min(g, nq));
+}
+
+apspie_status sssp_batch_grouped(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources, int32_t nq,
+                                 int32_t *d_dists, apspie_run_stats *stats) {
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (nq == 0) return APSPIE_OK;
+    const int m = A->m;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, reinterpret_cast<const void *>(sssp_group_kernel), kBlock, 0);
+    if (e != cudaSuccess || per_sm < 1) return cuda_error(ctx, e, "occupancy query");
+    const int cap = std::max(1, per_sm * ctx->num_sms / std::max(1, ctx->grid_share));
+    const int groups = std::min(sssp_group_count(ctx, nq), cap);
+    const int bpg = std::min(cap / groups, kMaxGrid);
+    void *base;
+    apspie_status st = scratch_reserve(ctx, sssp_group_scratch_need(m, groups), &base);
+    if (st != APSPIE_OK) return st;
+    if ((st = reset_ctl(ctx)) != APSPIE_OK) return st;
+    const size_t per = (trav_scratch_bytes(m) + 255) / 256 * 256;
+    TravCtl *ctls = reinterpret_cast<TravCtl *>(static_cast<char *>(base) + per * groups);
+    if ((e = cudaMemsetAsync(ctls, 0, groups * ((sizeof(TravCtl) + 255) / 256 * 256), ctx->stream)) != cudaSuccess)
+        return cuda_error(ctx, e, "apspie_sssp_batch reset");
+    SsspGroupArgs g;
+    SsspArgs &a = g.base;
+    std::memset(&a, 0, sizeof(a));
+    a.m = m;
+    a.nnz = A->nnz;
+    a.row_ptr = A->row_ptr;
+    a.col_ind = A->col_ind;
+    a.w = static_cast<const int *>(A->val);
+    const apspie_tune_params tp = effective_params(ctx, APSPIE_TUNE_SSSP, A);
+    a.delta_hint = tp.sssp_delta;
+    if (tp.sssp_band > 0) {
+        a.band = tp.sssp_band;
+    } else if (tp.sssp_band == 0) {
+        // the single-query default, scaled to the group's share of the device
+        long long b = A->nnz / 8;
+        b = b < (1LL << 18) ? (1LL << 18) : (b > (1LL << 23) ? (1LL << 23) : b);
+        b = b * bpg / cap;
+        a.band = b < (1LL << 16) ? (1LL << 16) : b;
+    } else {
+        a.band = 0;
+    }
+    a.is_float = 0;
+    a.unreached_bits = -1;
+    a.buf = carve_trav(base, m);
+    a.sticky = ctx->d_sticky_err;
+    g.srcs = d_sources;
+    g.out = d_dists;
+    g.nq = nq;
+    g.groups = groups;
+    g.m = m;
+    g.ctls = ctls;
+    g.buf_stride = per;
+    g.main = ctx->d_ctl;
+    void *args[] = {&g};
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(sssp_group_kernel), dim3(groups * bpg),
+                                    dim3(kBlock), args, 0, ctx->stream);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "cooperative launch");
+    return finish_call(ctx, stats, "apspie_sssp_batch");
+}
+
 }  // namespace apspie
 
 extern "C" {

@@ -218,6 +218,10 @@ class Context:
         """Edges expanded per SSSP iteration (lowest-distance band); 0 = auto, < 0 = off."""
         self._check(L.lib().apspie_ctx_set_sssp_band(self.handle, edges), "set_sssp_band")
 
+    def set_sssp_batch_groups(self, groups: int) -> None:
+        """Batched SSSP: 0 = 4 query groups, > 0 = that many, < 0 = the multi-query kernel."""
+        self._check(L.lib().apspie_ctx_set_sssp_batch_groups(self.handle, groups), "set_sssp_batch_groups")
+
     # ---- autotuner
     def get_params(self) -> dict:
         p = L.TuneParams()

@@ -96,15 +96,30 @@ def test_batch_rmat22_full_size(ctx):
 
 
 # ------------------------------------------------------------------ batched SSSP
+@pytest.mark.parametrize("groups", [0, 3, 64, -1])
 @pytest.mark.parametrize("nq", [1, 7, 32, 100, 512])
-def test_sssp_batch_rows_equal_single_sssp(ctx, rmat14, nq):
+def test_sssp_batch_rows_equal_single_sssp(ctx, rmat14, nq, groups):
+    """groups 0: the default 4 query groups; 3 / 64: that many (64 > 7 queries leaves
+    groups idle); -1: the multi-query kernel."""
     g, dg = rmat14
     s = _srcs(g, nq, 4)
-    out = ctx.sssp_batch(dg, s).cpu().numpy()
+    ctx.set_sssp_batch_groups(groups)
+    try:
+        out = ctx.sssp_batch(dg, s).cpu().numpy()
+        st = ctx.sssp_batch_into(dg, s, torch_empty_like_rows(nq, g.m), stats=True)
+    finally:
+        ctx.set_sssp_batch_groups(0)
+    assert st["edges_expanded"] > 0
     for q in sorted({0, nq // 2, nq - 1}):
         np.testing.assert_array_equal(out[q], oracle.sssp(g.row_ptr, g.col_ind, g.val, int(s[q])), err_msg=f"q{q}")
     for q in range(0, nq, max(1, nq // 8)):
         np.testing.assert_array_equal(out[q], ctx.sssp(dg, int(s[q])).cpu().numpy())
+
+
+def torch_empty_like_rows(nq, m):
+    import torch
+
+    return torch.empty((nq, m), dtype=torch.int32, device="cuda")
 
 
 def test_sssp_batch_duplicates_and_unreached(ctx, golden):
@@ -126,5 +141,5 @@ def test_sssp_batch_rmat20_full_size(ctx):
     dg = ap.DeviceGraph(g)
     s = torch.from_numpy(ap.lcc_sample(g, 64, 6)).cuda()
     out = ctx.sssp_batch(dg, s)
-    for q in (0, 63):
+    for q in (0, 17, 63):
         np.testing.assert_array_equal(out[q].cpu().numpy(), oracle.sssp(g.row_ptr, g.col_ind, g.val, int(s[q])))
