@@ -55,6 +55,7 @@ struct ExpandSmem {
     int qbuf[NWARP][2][QCAP];
     int base[kMaxGrid + 1];  // exclusive prefix of chunk totals
     int tsplit[BATCH + 1];   // merge-path split of each warp tile of the current batch
+    int next_tile;           // tiles of the batch handed out so far (warps take them in turn)
     int scan_tmp[33];
     Warp w[NWARP];
 };
@@ -182,8 +183,11 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
             if (d > total) d = total;
             sm.tsplit[s] = frontier_merge_path(d, nf, E, loc_off, sm.base, C);
         }
+        if (threadIdx.x == 0) sm.next_tile = NWARP;
         __syncthreads();
-        for (long long tile = tb + wid; tile < te; tile += NWARP) {
+        // a warp that finishes its tile takes the next unclaimed one, so tiles of uneven
+        // cost (atomics, queue flushes) do not leave warps idle at the batch's barrier
+        for (long long tile = tb + wid; tile < te;) {
             const long long d0 = tile * WT;
             const long long d1 = d0 + WT < total ? d0 + WT : total;
             const int a0 = sm.tsplit[tile - tb];
@@ -243,6 +247,9 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
             op(valid, kk, idx, ws);
             __syncwarp();
             post(ne, ws);
+            int nt = 0;
+            if (lane == 0) nt = atomicAdd(&sm.next_tile, 1);
+            tile = tb + __shfl_sync(0xffffffffu, nt, 0);
             __syncwarp();
         }
         __syncthreads();
