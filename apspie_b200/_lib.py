@@ -94,6 +94,7 @@ class ServerStats(ctypes.Structure):
 
 QUERY_BFS, QUERY_SSSP, QUERY_MIS = 0, 1, 2
 TUNE_BFS, TUNE_SSSP, TUNE_BFS_BATCH, TUNE_SPGEMM, TUNE_TC = 0, 1, 2, 3, 4
+BUILD_SYMMETRIZE, BUILD_DROP_SELF_LOOPS, BUILD_DEDUP = 1, 2, 4
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -140,6 +141,9 @@ SIGNATURES = {
     "apspie_csr_free": (None, [POINTER(CSROwned)]),
     "apspie_tc": (c_int, [c_void_p, POINTER(CSR), POINTER(c_int64)]),
     "apspie_csr_strict_lower_device": (c_int, [c_void_p, POINTER(CSR), POINTER(CSROwned)]),
+    "apspie_csr_build": (c_int, [c_void_p, c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_int32, c_int32,
+                                 POINTER(CSROwned)]),
+    "apspie_csr_transpose": (c_int, [c_void_p, POINTER(CSR), POINTER(CSROwned)]),
     # server
     "apspie_server_create": (c_int, [c_int, c_int64, c_int32, c_int32, POINTER(c_void_p)]),
     "apspie_server_add_graph": (c_int, [c_void_p, POINTER(HostCSR), c_int32, c_uint32, POINTER(c_int32)]),
@@ -157,6 +161,8 @@ SIGNATURES = {
     "apspie_gen_rmat": (c_int, [c_int, c_int, c_uint32, c_uint32, c_double, c_double, c_double,
                                 c_int, POINTER(HostCSR)]),
     "apspie_gen_er": (c_int, [c_int, c_int, c_uint32, c_int, POINTER(HostCSR)]),
+    "apspie_gen_rmat_coo": (c_int, [c_int, c_int, c_uint32, c_uint32, c_double, c_double, c_double, c_void_p,
+                                    c_void_p, c_void_p]),
     "apspie_mt19937_u32": (c_int, [c_uint32, c_int64, c_void_p]),
     "apspie_max_degree_vertex": (c_int32, [POINTER(HostCSR)]),
     "apspie_lcc_sample": (c_int, [POINTER(HostCSR), c_int32, c_uint32, c_void_p]),

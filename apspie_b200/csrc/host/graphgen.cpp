@@ -115,6 +115,31 @@ void apspie_host_csr_free(apspie_host_csr *g) {
     g->val = nullptr;
 }
 
+apspie_status apspie_gen_rmat_coo(int scale, int edge_factor, uint32_t seed, uint32_t weight_seed, double a,
+                                  double b, double c, int32_t *src, int32_t *dst, int32_t *weight) {
+    if (!src || !dst || scale < 1 || scale > 30 || edge_factor < 1) return APSPIE_ERR_INVALID_ARG;
+    const int64_t ne = (int64_t(1) << scale) * edge_factor;
+    if (ne > INT32_MAX) return APSPIE_ERR_UNSUPPORTED;
+    const double ab = a + b, abc = a + b + c;
+    std::mt19937 rng(seed);
+    std::uniform_real_distribution<double> U(0.0, 1.0);
+    std::mt19937 wrng(weight_seed);
+    std::uniform_int_distribution<int> W(1, 255);
+    for (int64_t k = 0; k < ne; ++k) {
+        uint32_t u = 0, v = 0;
+        for (int l = 0; l < scale; ++l) {
+            const double r = U(rng);
+            u = (u << 1) | ((r >= ab) ? 1u : 0u);
+            v = (v << 1) | ((r < a) ? 0u : (r < ab ? 1u : (r < abc ? 0u : 1u)));
+        }
+        const int wk = W(wrng);
+        src[k] = static_cast<int32_t>(u);
+        dst[k] = static_cast<int32_t>(v);
+        if (weight) weight[k] = wk;
+    }
+    return APSPIE_OK;
+}
+
 apspie_status apspie_gen_rmat(int scale, int edge_factor, uint32_t seed, uint32_t weight_seed,
                               double a, double b, double c, int with_weights,
                               apspie_host_csr *out) {

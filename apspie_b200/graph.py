@@ -93,6 +93,19 @@ def gen_rmat(scale: int, edge_factor: int = 16, seed: int = 1, weight_seed: int 
     return _from_struct(s, symmetric=True)
 
 
+def gen_rmat_coo(scale: int, edge_factor: int = 16, seed: int = 1, weight_seed: int = 3,
+                 a: float = 0.57, b: float = 0.19, c: float = 0.19):
+    """The R-MAT edge list in generation order (self-loops and repeats included):
+    (src, dst, weight) int32 arrays."""
+    ne = (1 << scale) * edge_factor
+    src = np.empty(ne, dtype=np.int32)
+    dst = np.empty(ne, dtype=np.int32)
+    w = np.empty(ne, dtype=np.int32)
+    L.check(L.lib().apspie_gen_rmat_coo(scale, edge_factor, seed, weight_seed, a, b, c, src.ctypes.data,
+                                        dst.ctypes.data, w.ctypes.data), None, "gen_rmat_coo")
+    return src, dst, w
+
+
 def gen_er(n: int, k: int = 8, seed: int = 5, val_type: int = L.VAL_F32) -> HostGraph:
     s = L.HostCSR()
     L.check(L.lib().apspie_gen_er(n, k, seed, val_type, ctypes.byref(s)), None, "gen_er")
@@ -391,6 +404,26 @@ class Context:
         out = ctypes.c_int64()
         self._check(L.lib().apspie_tc(self.handle, ctypes.byref(Lg.view(False)), ctypes.byref(out)), "tc")
         return int(out.value)
+
+    def build_csr(self, m: int, src, dst, val=None, flags: int = 0) -> "OwnedDeviceCSR":
+        """Device COO (int32 CUDA tensors; val int32 or float32 or None) -> CSR, see
+        apspie_csr_build (flags: BUILD_SYMMETRIZE | BUILD_DROP_SELF_LOOPS | BUILD_DEDUP)."""
+        import torch
+
+        vt = L.VAL_NONE if val is None else (L.VAL_F32 if val.dtype == torch.float32 else L.VAL_I32)
+        C = L.CSROwned()
+        self._check(L.lib().apspie_csr_build(self.handle, m, int(src.shape[0]), src.data_ptr(), dst.data_ptr(),
+                                             val.data_ptr() if val is not None else None, vt, flags,
+                                             ctypes.byref(C)), "csr_build")
+        out = OwnedDeviceCSR(C)
+        out.symmetric = bool(flags & L.BUILD_SYMMETRIZE)
+        return out
+
+    def transpose(self, A) -> "OwnedDeviceCSR":
+        C = L.CSROwned()
+        self._check(L.lib().apspie_csr_transpose(self.handle, ctypes.byref(A.view(True)), ctypes.byref(C)),
+                    "csr_transpose")
+        return OwnedDeviceCSR(C)
 
     def strict_lower(self, A: DeviceGraph) -> "OwnedDeviceCSR":
         C = L.CSROwned()

@@ -287,6 +287,30 @@ apspie_status apspie_spgemm_numeric(apspie_ctx *ctx, const apspie_csr *A, const 
                                     const int32_t *d_row_ptr_c, int32_t *d_col_c, void *d_val_c);
 void apspie_csr_free(apspie_csr_owned *C);
 
+/* ---- graph construction on the device ---------------------------------------------- */
+
+enum {
+    APSPIE_BUILD_SYMMETRIZE = 1,       /* store {u, v} in both rows (canonical pair lo < hi) */
+    APSPIE_BUILD_DROP_SELF_LOOPS = 2,  /* drop edges u == v */
+    APSPIE_BUILD_DEDUP = 4             /* keep the first occurrence of each pair (input order) */
+};
+
+/* Builds a CSR with sorted rows from nedges device COO edges (d_src[k], d_dst[k], optional
+ * 32-bit values d_val[k] of val_type). With SYMMETRIZE | DROP_SELF_LOOPS | DEDUP it applies
+ * the rules of the host R-MAT generator and makeSymmetric: self-loops dropped, each
+ * unordered pair kept once with the value of its first occurrence, then mirrored; row r
+ * lists its lower neighbours then its upper ones, ascending. The output is allocated by
+ * the callee (apspie_csr_free). Replaces makeSymmetric + buildMatrix
+ * (src/util.cuh:573-643, src/matrix.cpp:55-111) for graphs already in device memory.
+ * Synchronises. */
+apspie_status apspie_csr_build(apspie_ctx *ctx, int32_t m, int64_t nedges, const int32_t *d_src,
+                               const int32_t *d_dst, const void *d_val, int32_t val_type, int32_t flags,
+                               apspie_csr_owned *out);
+/* CSR -> CSC (the transpose as a CSR of n rows), rows sorted; values follow their entries.
+ * Replaces csr2csc (src/util.cuh:474) and extract_csr2csc (src/matrix.cpp:229).
+ * Synchronises. */
+apspie_status apspie_csr_transpose(apspie_ctx *ctx, const apspie_csr *A, apspie_csr_owned *out);
+
 /* Triangle count = sum((L*L) .* L) for L the strict lower triangle (column < row) of a
  * symmetric graph, rows sorted; masked hash SpGEMM, L*L never materialised; int64 result
  * (synchronises). Replaces the flow of test/tc/main.cu:243-249 (spgemm<T> tc.cuh:63 ->

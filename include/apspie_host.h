@@ -46,6 +46,12 @@ apspie_status apspie_load_mtx(const char *path, int undirected, apspie_host_csr 
 apspie_status apspie_gen_rmat(int scale, int edge_factor, uint32_t seed, uint32_t weight_seed,
                               double a, double b, double c, int with_weights,
                               apspie_host_csr *out);
+/* The generated edge list itself, in generation order, before self-loops are dropped and
+ * pairs deduplicated: src/dst/weight[k] for k < 2^scale * edge_factor (weight may be NULL).
+ * apspie_csr_build with SYMMETRIZE | DROP_SELF_LOOPS | DEDUP turns it into exactly the CSR
+ * apspie_gen_rmat returns. */
+apspie_status apspie_gen_rmat_coo(int scale, int edge_factor, uint32_t seed, uint32_t weight_seed, double a,
+                                  double b, double c, int32_t *src, int32_t *dst, int32_t *weight);
 
 /* Erdos-Renyi matrix with exactly k distinct uniformly random columns per row: row by row,
  * draws of std::mt19937(seed) through std::uniform_int_distribution<int>(0, n-1), repeats
