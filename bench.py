@@ -247,6 +247,8 @@ def main_ours(args, ws, rank, local):
         ctx = ap.Context(local)
         if args.only_extra == "spgemm_tc":
             res = extras_spgemm_tc(ctx, args, ws, local)
+        elif args.only_extra == "build":
+            res = extras_build(ctx, args, ws, local)
         else:
             g22 = ap.gen_rmat(22, 16, 1, 3)
             res = extras_batched(ctx, args, ws, local, g22) if args.only_extra == "batched" \
@@ -420,10 +422,45 @@ def extras(ctx, args, ws, local):
                          "pull_levels": st["pull_iterations"]}
     del d20, o20, mem, prio
     res.update(extras_spgemm_tc(ctx, args, ws, local))
+    res.update(extras_build(ctx, args, ws, local))
     g22 = ap.gen_rmat(22, 16, 1, 3)  # weights for the serving leg; BFS ignores them
     res.update(extras_batched(ctx, args, ws, local, g22))
     if ws == 1:
         res.update(extras_serving(ctx, args, local, g22))
+    return res
+
+
+def extras_build(ctx, args, ws, local):
+    """Device graph construction: the R-MAT scale-20 edge list (seed 2, 16.8M generated
+    edges with self-loops and repeats) -> symmetrised, deduplicated, weighted CSR; and the
+    transpose of the ER n=2^20 matrix. Checked against the host generator's CSR."""
+    import torch
+
+    import apspie_b200 as ap
+
+    dev = f"cuda:{local}"
+    src, dst, w = ap.gen_rmat_coo(20, 16, 2, 3)
+    ds, dd, dw = (torch.from_numpy(x).to(dev) for x in (src, dst, w))
+    flags = ap.BUILD_SYMMETRIZE | ap.BUILD_DROP_SELF_LOOPS | ap.BUILD_DEDUP
+    for _ in range(2):
+        C = ctx.build_csr(1 << 20, ds, dd, dw, flags)
+        C.free()
+    steps = 5
+    tot, _ = time_steps(ctx.stream, lambda: ctx.build_csr(1 << 20, ds, dd, dw, flags).free(), steps)
+    ms = max_over_ranks(ws, tot / steps)
+    C = ctx.build_csr(1 << 20, ds, dd, dw, flags)
+    rp, ci, val = C.to_numpy()
+    g = ap.gen_rmat(20, 16, 2, 3)
+    exact = bool(np.array_equal(rp, g.row_ptr) and np.array_equal(ci, g.col_ind) and np.array_equal(val, g.val))
+    res = {"csr_build_rmat20": {"ms": ms, "edges_in": int(src.shape[0]), "nnz_out": int(C.nnz),
+                                "Gedges_per_s": src.shape[0] / (ms * 1e-3) / 1e9, "exact": exact}}
+    C.free()
+    e = ap.gen_er(1 << 20, 8, 5, ap.VAL_F32)
+    A = ap.DeviceGraph(e, dev)
+    for _ in range(2):
+        ctx.transpose(A).free()
+    tot, _ = time_steps(ctx.stream, lambda: ctx.transpose(A).free(), steps)
+    res["transpose_er20"] = {"ms": max_over_ranks(ws, tot / steps), "nnz": e.nnz}
     return res
 
 
@@ -666,7 +703,7 @@ def main():
     ap_.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap_.add_argument("--no-extra", action="store_true")
     ap_.add_argument("--no-cpu-baseline", action="store_true")
-    ap_.add_argument("--only-extra", choices=["spgemm_tc", "batched", "serving"], default=None,
+    ap_.add_argument("--only-extra", choices=["spgemm_tc", "build", "batched", "serving"], default=None,
                      help="run one extra leg alone and print its JSON (no headline line)")
     args = ap_.parse_args()
     ws, rank, local = dist_env()
