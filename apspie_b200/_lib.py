@@ -144,6 +144,8 @@ SIGNATURES = {
     "apspie_csr_build": (c_int, [c_void_p, c_int32, c_int64, c_void_p, c_void_p, c_void_p, c_int32, c_int32,
                                  POINTER(CSROwned)]),
     "apspie_csr_transpose": (c_int, [c_void_p, POINTER(CSR), POINTER(CSROwned)]),
+    "apspie_spmv": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p, c_float, c_float]),
+    "apspie_pagerank": (c_int, [c_void_p, POINTER(CSR), c_float, c_double, c_int32, c_void_p, POINTER(c_int32)]),
     # server
     "apspie_server_create": (c_int, [c_int, c_int64, c_int32, c_int32, POINTER(c_void_p)]),
     "apspie_server_add_graph": (c_int, [c_void_p, POINTER(HostCSR), c_int32, c_uint32, POINTER(c_int32)]),

@@ -419,6 +419,21 @@ class Context:
         out.symmetric = bool(flags & L.BUILD_SYMMETRIZE)
         return out
 
+    def spmv_into(self, A, x, y, alpha: float = 1.0, beta: float = 0.0) -> None:
+        """y = alpha * A x + beta * y (float32 CUDA tensors)."""
+        self._check(L.lib().apspie_spmv(self.handle, ctypes.byref(A.view(True)), x.data_ptr(), y.data_ptr(),
+                                        alpha, beta), "spmv")
+
+    def pagerank(self, A, damping: float = 0.85, tol: float = 1e-6, max_iter: int = 100):
+        """(rank float32 CUDA tensor, iterations)."""
+        import torch
+
+        r = torch.empty(A.m, dtype=torch.float32, device=f"cuda:{self.device}")
+        it = ctypes.c_int32()
+        self._check(L.lib().apspie_pagerank(self.handle, ctypes.byref(A.view(False)), damping, tol, max_iter,
+                                            r.data_ptr(), ctypes.byref(it)), "pagerank")
+        return r, it.value
+
     def transpose(self, A) -> "OwnedDeviceCSR":
         C = L.CSROwned()
         self._check(L.lib().apspie_csr_transpose(self.handle, ctypes.byref(A.view(True)), ctypes.byref(C)),

@@ -311,6 +311,22 @@ apspie_status apspie_csr_build(apspie_ctx *ctx, int32_t m, int64_t nedges, const
  * Synchronises. */
 apspie_status apspie_csr_transpose(apspie_ctx *ctx, const apspie_csr *A, apspie_csr_owned *out);
 
+/* ---- dense-vector SpMV and PageRank -------------------------------------------------- */
+
+/* y = alpha * A * x + beta * y (float32; A with float32 values, or a pattern of 1.0s).
+ * Replaces SpmvCsrBinary (src/bfs.cuh:11-14) and cuspmv (src/tc.cuh:17-59). */
+apspie_status apspie_spmv(apspie_ctx *ctx, const apspie_csr *A, const float *d_x, float *d_y, float alpha,
+                          float beta);
+/* PageRank of the directed graph A (row u lists u's out-edges): r = 1/n initially, then
+ * r' = (1 - damping) / n + damping * (sum over in-edges (u, v) of r[u] / outdeg(u)
+ * + (rank mass of vertices without out-edges) / n), until sum |r' - r| < tol or max_iter
+ * iterations (*iterations reports how many ran). d_rank: float32[m], so a tol below what
+ * float32 ranks resolve (about 1e-7 summed over the graph) runs all max_iter iterations.
+ * Synchronises once per iteration. No reference counterpart (the reference ships
+ * test_pr.mtx only). */
+apspie_status apspie_pagerank(apspie_ctx *ctx, const apspie_csr *A, float damping, double tol, int32_t max_iter,
+                              float *d_rank, int32_t *iterations);
+
 /* Triangle count = sum((L*L) .* L) for L the strict lower triangle (column < row) of a
  * symmetric graph, rows sorted; masked hash SpGEMM, L*L never materialised; int64 result
  * (synchronises). Replaces the flow of test/tc/main.cu:243-249 (spgemm<T> tc.cuh:63 ->

@@ -138,6 +138,40 @@ def tc(row_ptr_l, col_ind_l):
     return int(lib().oracle_tc(rp.shape[0] - 1, _p(rp), _p(ci)))
 
 
+def spmv(row_ptr, col_ind, val, x):
+    """y = A x in float64 (val None: a pattern of 1.0s); the dense-vector product of
+    cuspmv (src/tc.cuh:17-59) and SpmvCsrBinary (src/bfs.cuh:11-14)."""
+    rp = np.asarray(row_ptr, dtype=np.int64)
+    rows = np.repeat(np.arange(rp.shape[0] - 1), np.diff(rp))
+    a = np.ones(rows.shape[0]) if val is None else np.asarray(val, dtype=np.float64)
+    y = np.zeros(rp.shape[0] - 1)
+    np.add.at(y, rows, a * np.asarray(x, dtype=np.float64)[np.asarray(col_ind, dtype=np.int64)])
+    return y
+
+
+def pagerank(row_ptr, col_ind, damping=0.85, tol=1e-6, max_iter=100):
+    """Power iteration in float64: r = 1/n, r' = (1 - d)/n + d (sum over in-edges of
+    r[u]/outdeg(u) + dangling mass / n), until sum |r' - r| < tol. Returns (r, iterations)."""
+    rp = np.asarray(row_ptr, dtype=np.int64)
+    n = rp.shape[0] - 1
+    deg = np.diff(rp)
+    rows = np.repeat(np.arange(n), deg)
+    cols = np.asarray(col_ind, dtype=np.int64)
+    r = np.full(n, 1.0 / n)
+    it = 0
+    while it < max_iter:
+        x = np.where(deg > 0, r / np.maximum(deg, 1), 0.0)
+        y = np.zeros(n)
+        np.add.at(y, cols, x[rows])
+        nr = (1.0 - damping) / n + damping * (y + r[deg == 0].sum() / n)
+        diff = np.abs(nr - r).sum()
+        r = nr
+        it += 1
+        if diff < tol:
+            break
+    return r, it
+
+
 def mt19937(seed, count):
     out = np.empty(count, dtype=np.uint32)
     lib().oracle_mt19937(int(seed), int(count), _p(out))

@@ -222,3 +222,15 @@ def test_reference_driver_agrees_on_rmat14():
     np.testing.assert_array_equal(oracle.ref_bfs(g.row_ptr, g.col_ind, src)[0], oracle.bfs(g.row_ptr, g.col_ind, src))
     np.testing.assert_array_equal(oracle.ref_sssp(g.row_ptr, g.col_ind, g.val, src)[0],
                                   oracle.sssp(g.row_ptr, g.col_ind, g.val, src))
+
+
+def test_oracle_pagerank_and_spmv_sanity():
+    # a directed 4-cycle: every vertex has rank 1/4; a star's centre collects the most rank
+    rp = np.array([0, 1, 2, 3, 4]); ci = np.array([1, 2, 3, 0])
+    r, it = oracle.pagerank(rp, ci, 0.85, 1e-12, 100)
+    np.testing.assert_allclose(r, 0.25)
+    rp = np.array([0, 1, 2, 3, 3]); ci = np.array([3, 3, 3])  # three leaves -> sink 3 (dangling)
+    r, _ = oracle.pagerank(rp, ci, 0.85, 1e-12, 500)
+    assert abs(r.sum() - 1.0) < 1e-12 and r[3] > r[0]
+    np.testing.assert_allclose(oracle.spmv(np.array([0, 2, 3]), np.array([0, 1, 1]), np.array([1.0, 2.0, 3.0]),
+                                           np.array([1.0, 10.0])), [21.0, 30.0])
