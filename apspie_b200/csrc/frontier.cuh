@@ -156,8 +156,9 @@ __device__ __forceinline__ int frontier_merge_path(long long diag, int nf, int E
 // Phase B. load(j, k, ws) stages entry j's payload into the warp slice at k;
 // op(valid, k, idx, ws) handles a lane's VT edges (CSR positions idx[], owning staged
 // entries k[]); post(ne, ws) runs after the tile's edges (per-entry flushes). All three
-// are called by every lane of the warp, so they may use warp collectives.
-template <int BLOCK, int VT, bool EXTRA, class Load, class Op, class Post>
+// are called by every lane of the warp, so they may use warp collectives. DYN: warps claim
+// the tiles of their block's batch in turn (else tile i goes to warp i % NWARP).
+template <int BLOCK, int VT, bool EXTRA, bool DYN = true, class Load, class Op, class Post>
 __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__restrict__ loc_off,
                                                 const int *__restrict__ rs,
                                                 ExpandSmem<BLOCK, VT, EXTRA> &sm, Load load, Op op,
@@ -247,9 +248,13 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
             op(valid, kk, idx, ws);
             __syncwarp();
             post(ne, ws);
-            int nt = 0;
-            if (lane == 0) nt = atomicAdd(&sm.next_tile, 1);
-            tile = tb + __shfl_sync(0xffffffffu, nt, 0);
+            if (DYN) {
+                int nt = 0;
+                if (lane == 0) nt = atomicAdd(&sm.next_tile, 1);
+                tile = tb + __shfl_sync(0xffffffffu, nt, 0);
+            } else {
+                tile += NWARP;
+            }
             __syncwarp();
         }
         __syncthreads();
