@@ -137,6 +137,10 @@ apspie_status finish_call(apspie_ctx *ctx, apspie_run_stats *stats, const char *
 size_t traversal_scratch_need(int m);        // apspie_bfs / apspie_sssp
 size_t mis_scratch_need(int m);              // apspie_mis
 size_t bfs_batch_scratch_need(int m, int nq);  // apspie_bfs_batch (nq <= 512 per launch)
+// apspie_bfs_batch into per-query rows h_rows[q] (host array of device pointers) when
+// h_rows is given, else into the query-major d_depths
+apspie_status bfs_batch_impl(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources, int32_t num_sources,
+                             int32_t depth_cap, int32_t *d_depths, int32_t *const *h_rows, apspie_run_stats *stats);
 size_t sssp_batch_scratch_need(int m, int nq);  // apspie_sssp_batch (nq <= 512 per launch)
 // apspie_sssp_batch in query groups (each group of blocks runs single-source SSSPs)
 size_t sssp_group_scratch_need(int m, int groups);

@@ -40,7 +40,8 @@ struct MsArgs {
     const int *__restrict__ row_ptr;
     const int *__restrict__ col_ind;
     const int *__restrict__ srcs;
-    int *out;             // nq x m, pre-filled with -1
+    int *out;             // nq x m, pre-filled with -1 (when rows is null)
+    int *const *rows;     // else: query q's depths go to rows[q][0..m), pre-filled with -1
     unsigned *vis;        // m x W
     unsigned *fr[2];      // m x W each
     unsigned *touched;    // m bits
@@ -52,6 +53,10 @@ struct MsArgs {
     int *sticky;
     float push_frac;      // push while |active| * mean degree < push_frac * nnz
 };
+
+__device__ __forceinline__ int *depth_row(const MsArgs &a, int q) {
+    return a.rows ? a.rows[q] : a.out + static_cast<long long>(q) * a.m;
+}
 
 // Bits of word w that belong to real queries (0..nq-1).
 __device__ __forceinline__ unsigned query_mask(int nq, int w) {
@@ -113,7 +118,7 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
                 const unsigned bit = 1u << (qi & 31);
                 atomicOr(a.vis + static_cast<long long>(v) * W + (qi >> 5), bit);
                 atomicOr(a.fr[0] + static_cast<long long>(v) * W + (qi >> 5), bit);
-                a.out[static_cast<long long>(qi) * m + v] = 0;
+                depth_row(a, qi)[v] = 0;
                 const unsigned tb = 1u << (v & 31);
                 first = !(atomicOr(a.touched + (v >> 5), tb) & tb);
             }
@@ -225,7 +230,7 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
                             while (b) {
                                 const int bit = __ffs(b) - 1;
                                 b &= b - 1;
-                                a.out[static_cast<long long>(w * 32 + bit) * m + v] = L + 1;
+                                depth_row(a, w * 32 + bit)[v] = L + 1;
                             }
                         }
                     }
@@ -301,7 +306,7 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
                     while (anyb) {
                         const int bit = __ffs(anyb) - 1;
                         anyb &= anyb - 1;
-                        if ((got[w] >> bit) & 1u) a.out[static_cast<long long>(w * 32 + bit) * m + v] = L + 1;
+                        if ((got[w] >> bit) & 1u) depth_row(a, w * 32 + bit)[v] = L + 1;
                     }
                 }
                 aw.push(any, v);
@@ -359,7 +364,7 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
                             while (b) {
                                 const int bit = __ffs(b) - 1;
                                 b &= b - 1;
-                                a.out[static_cast<long long>(threadIdx.x * 32 + bit) * m + v] = L + 1;
+                                depth_row(a, threadIdx.x * 32 + bit)[v] = L + 1;
                             }
                         }
                     }
@@ -410,16 +415,20 @@ size_t bfs_batch_scratch_need(int m, int nq) { return batch_need(m, padded_words
 
 using namespace apspie;
 
-extern "C" apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources,
-                                          int32_t num_sources, int32_t depth_cap, int32_t *d_depths,
-                                          apspie_run_stats *stats) {
+namespace apspie {
+
+// The batched BFS with either a query-major output (d_depths) or, when h_rows is given, one
+// output row per query (h_rows[q], device pointers): the server writes each answer straight
+// into its request's buffer this way.
+apspie_status bfs_batch_impl(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources, int32_t num_sources,
+                             int32_t depth_cap, int32_t *d_depths, int32_t *const *h_rows, apspie_run_stats *stats) {
     if (!ctx) return APSPIE_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     apspie_status st = check_csr_view(ctx, A, "apspie_bfs_batch");
     if (st != APSPIE_OK) return st;
     if (A->m != A->n || A->m <= 0)
         return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_bfs_batch: square, non-empty graph required");
-    if (num_sources < 0 || (num_sources > 0 && (!d_sources || !d_depths)))
+    if (num_sources < 0 || (num_sources > 0 && (!d_sources || (!d_depths && !h_rows))))
         return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_bfs_batch: bad sources/output");
     if (ctx->validate && (st = validate_csr(ctx, A, true)) != APSPIE_OK) return st;
     const int m = A->m;
@@ -432,10 +441,11 @@ extern "C" apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, 
         const size_t mw = static_cast<size_t>(m) * Wp;
         const size_t words = (static_cast<size_t>(m) + 31) / 32;
         void *base;
-        st = scratch_reserve(ctx, batch_need(m, Wp), &base);
+        st = scratch_reserve(ctx, batch_need(m, Wp) + (h_rows ? Carver::need({kMaxQ * sizeof(int *)}) : 0), &base);
         if (st != APSPIE_OK) return st;
         Carver c(base);
         MsArgs a;
+        a.rows = nullptr;
         a.vis = c.take<unsigned>(mw);
         a.fr[0] = c.take<unsigned>(mw);
         a.fr[1] = c.take<unsigned>(mw);
@@ -455,14 +465,25 @@ extern "C" apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, 
         a.row_ptr = A->row_ptr;
         a.col_ind = A->col_ind;
         a.srcs = d_sources + q0;
-        a.out = d_depths + static_cast<size_t>(q0) * m;
+        a.out = d_depths ? d_depths + static_cast<size_t>(q0) * m : nullptr;
         a.ctl = ctx->d_ctl;
         a.sticky = ctx->d_sticky_err;
         // pull levels scan a vertex's own row for parents: valid for symmetric patterns only
         a.push_frac = (A->flags & APSPIE_CSR_SYMMETRIC)
                           ? effective_params(ctx, APSPIE_TUNE_BFS_BATCH, A).batch_push_frac
                           : 1e30f;
-        cudaError_t e = cudaMemsetAsync(a.out, 0xff, static_cast<size_t>(nq) * m * sizeof(int32_t), ctx->stream);
+        cudaError_t e = cudaSuccess;
+        if (h_rows) {
+            int32_t **table = c.take<int32_t *>(kMaxQ);
+            // pageable source: the copy is staged before the call returns
+            e = cudaMemcpyAsync(table, h_rows + q0, static_cast<size_t>(nq) * sizeof(int32_t *),
+                                cudaMemcpyHostToDevice, ctx->stream);
+            for (int q = 0; q < nq && e == cudaSuccess; ++q)
+                e = cudaMemsetAsync(h_rows[q0 + q], 0xff, static_cast<size_t>(m) * sizeof(int32_t), ctx->stream);
+            a.rows = table;
+        } else {
+            e = cudaMemsetAsync(a.out, 0xff, static_cast<size_t>(nq) * m * sizeof(int32_t), ctx->stream);
+        }
         if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(TravCtl), ctx->stream);
         if (e != cudaSuccess) return cuda_error(ctx, e, "apspie_bfs_batch reset");
         const void *fn = Wp == 1 ? msbfs_fn<1>() : Wp == 2 ? msbfs_fn<2>() : Wp == 4 ? msbfs_fn<4>()
@@ -479,4 +500,14 @@ extern "C" apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, 
         }
     }
     return APSPIE_OK;
+}
+
+}  // namespace apspie
+
+extern "C" apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources,
+                                          int32_t num_sources, int32_t depth_cap, int32_t *d_depths,
+                                          apspie_run_stats *stats) {
+    if (ctx && num_sources > 0 && !d_depths)
+        return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_bfs_batch: bad sources/output");
+    return bfs_batch_impl(ctx, A, d_sources, num_sources, depth_cap, d_depths, nullptr, stats);
 }

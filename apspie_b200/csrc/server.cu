@@ -7,8 +7,8 @@
 // slots overlap on the device). Whenever a slot is free it takes the (graph, kind) whose
 // oldest pending request is oldest and folds every request of that pair that is waiting
 // at that moment into one launch:
-//   BFS  -> apspie_bfs_batch over up to max_batch sources, rows copied device-to-device
-//           into each request's output buffer; fewer than bfs_min_batch waiting requests
+//   BFS  -> the batched BFS over up to max_batch sources, each depth row written straight
+//           into its request's output buffer; fewer than bfs_min_batch waiting requests
 //           (6 by default) run apspie_bfs each instead, which is faster for so few;
 //   MIS  -> one apspie_mis (the fixed priorities make every MIS query on a graph the same
 //           question), the set copied to every waiting request;
@@ -115,12 +115,14 @@ bool batched(int kind, int n, int bfs_min) {
 size_t arena_need(const apspie_csr &g, int kind, int n, int bfs_min) {
     if (kind == APSPIE_QUERY_MIS) return mis_scratch_need(g.m);
     if (!batched(kind, n, bfs_min)) return traversal_scratch_need(g.m);
-    return kind == APSPIE_QUERY_BFS ? bfs_batch_scratch_need(g.m, n) : sssp_batch_scratch_need(g.m, n);
+    return kind == APSPIE_QUERY_BFS ? bfs_batch_scratch_need(g.m, n) + 8192  // + the row-pointer table
+                                    : sssp_batch_scratch_need(g.m, n);
 }
 
-// Batched launches stage their n rows before copying them out.
+// Batched SSSP launches stage their n rows before copying them out (batched BFS writes
+// straight into the requests' buffers).
 size_t stage_need(const apspie_csr &g, int kind, int n, int bfs_min) {
-    return batched(kind, n, bfs_min) ? static_cast<size_t>(n) * g.m * 4 : 0;
+    return kind == APSPIE_QUERY_SSSP && batched(kind, n, bfs_min) ? static_cast<size_t>(n) * g.m * 4 : 0;
 }
 
 // Device bytes a slot holds now (its arena never shrinks; staging is kept for reuse).
@@ -172,7 +174,8 @@ void launch_batch(apspie_server *s, Slot &sl) {
     } else if (sl.kind == APSPIE_QUERY_BFS || sl.kind == APSPIE_QUERY_SSSP) {
         std::vector<int32_t> srcs(n);
         for (int i = 0; i < n; ++i) srcs[i] = sl.batch[i].source;
-        const size_t rows = static_cast<size_t>(n) * g.view.m * sizeof(int32_t);
+        const bool staged_rows = sl.kind == APSPIE_QUERY_SSSP;  // BFS writes into the requests' rows
+        const size_t rows = staged_rows ? static_cast<size_t>(n) * g.view.m * sizeof(int32_t) : 0;
         if (sl.stage_cap < rows) {
             cudaStreamSynchronize(sl.stream);
             if (sl.stage) cudaFree(sl.stage);
@@ -201,11 +204,15 @@ void launch_batch(apspie_server *s, Slot &sl) {
             cudaMemcpyAsync(sl.d_src, srcs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, sl.stream);
             // the host vector must outlive the copy
             cudaStreamSynchronize(sl.stream);
-            st = sl.kind == APSPIE_QUERY_BFS
-                     ? apspie_bfs_batch(sl.ctx, &g.view, sl.d_src, n, 0, static_cast<int32_t *>(sl.stage), nullptr)
-                     : apspie_sssp_batch(sl.ctx, &g.view, sl.d_src, n, static_cast<int32_t *>(sl.stage), nullptr);
+            if (sl.kind == APSPIE_QUERY_BFS) {
+                std::vector<int32_t *> out(n);
+                for (int i = 0; i < n; ++i) out[i] = static_cast<int32_t *>(sl.batch[i].d_out);
+                st = bfs_batch_impl(sl.ctx, &g.view, sl.d_src, n, 0, nullptr, out.data(), nullptr);
+            } else {
+                st = apspie_sssp_batch(sl.ctx, &g.view, sl.d_src, n, static_cast<int32_t *>(sl.stage), nullptr);
+            }
         }
-        if (st == APSPIE_OK)
+        if (st == APSPIE_OK && staged_rows)
             for (int i = 0; i < n; ++i)
                 cudaMemcpyAsync(sl.batch[i].d_out, static_cast<char *>(sl.stage) + static_cast<size_t>(i) * g.view.m * 4,
                                 static_cast<size_t>(g.view.m) * 4, cudaMemcpyDeviceToDevice, sl.stream);
@@ -384,11 +391,26 @@ apspie_status apspie_server_set_bfs_min_batch(apspie_server *s, int32_t min_batc
 apspie_status apspie_server_start(apspie_server *s) {
     if (!s || s->started) return APSPIE_ERR_INVALID_ARG;
     if (s->graph_bytes + s->slot_reserve * s->slots.size() > static_cast<size_t>(s->budget)) return APSPIE_ERR_OOM;
-    // reserve each slot's scratch up front so admission accounting matches the device
+    // reserve each slot's scratch up front so admission accounting matches the device: the
+    // largest launch (a full batch on the largest graph) when the budget allows it, so no
+    // arena grows (with a device synchronisation) while requests wait; else the
+    // single-query need, and batches then grow it only as far as the budget lets them
     int32_t mmax = 0;
     for (auto &g : s->graphs) mmax = std::max(mmax, g.view.m);
-    for (auto &sl : s->slots)
-        if (apspie_ctx_reserve(sl.ctx, mmax, 0) != APSPIE_OK) return APSPIE_ERR_OOM;
+    size_t full = traversal_scratch_need(mmax);
+    if (mmax > 0) {
+        full = std::max(full, mis_scratch_need(mmax));
+        full = std::max(full, bfs_batch_scratch_need(mmax, s->max_batch) + 8192);
+        if (s->sssp_fold > 1) full = std::max(full, sssp_batch_scratch_need(mmax, s->sssp_fold));
+    }
+    const size_t with_headroom = full + full / 8;
+    const bool fits = s->graph_bytes + with_headroom * s->slots.size() <= static_cast<size_t>(s->budget);
+    for (auto &sl : s->slots) {
+        void *base;
+        const apspie_status st =
+            fits ? scratch_reserve(sl.ctx, full, &base) : apspie_ctx_reserve(sl.ctx, mmax, 0);
+        if (st != APSPIE_OK) return APSPIE_ERR_OOM;
+    }
     s->started = true;
     s->worker = std::thread(worker_loop, s);
     return APSPIE_OK;
