@@ -160,6 +160,7 @@ SIGNATURES = {
     # host graph construction
     "apspie_host_csr_free": (None, [POINTER(HostCSR)]),
     "apspie_load_mtx": (c_int, [c_char_p, c_int, POINTER(HostCSR)]),
+    "apspie_load_mtx_threads": (c_int, [c_char_p, c_int, c_int, POINTER(HostCSR)]),
     "apspie_gen_rmat": (c_int, [c_int, c_int, c_uint32, c_uint32, c_double, c_double, c_double,
                                 c_int, POINTER(HostCSR)]),
     "apspie_gen_er": (c_int, [c_int, c_int, c_uint32, c_int, POINTER(HostCSR)]),

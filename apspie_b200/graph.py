@@ -78,10 +78,15 @@ def _from_struct(s: L.HostCSR, symmetric: bool = False) -> HostGraph:
     return HostGraph(m, n, rp, ci, val, symmetric)
 
 
-def load_mtx(path: str, undirected: bool) -> HostGraph:
+def load_mtx(path: str, undirected: bool, threads: Optional[int] = None) -> HostGraph:
+    """Matrix Market file -> CSR with the reference loader's semantics; threads (0 = all)
+    selects the parallel parser, None the single-threaded one."""
     s = L.HostCSR()
-    L.check(L.lib().apspie_load_mtx(path.encode(), int(undirected), ctypes.byref(s)), None,
-            f"load_mtx({path})")
+    if threads is None:
+        st = L.lib().apspie_load_mtx(str(path).encode(), int(undirected), ctypes.byref(s))
+    else:
+        st = L.lib().apspie_load_mtx_threads(str(path).encode(), int(undirected), int(threads), ctypes.byref(s))
+    L.check(st, None, f"load_mtx({path})")
     return _from_struct(s, symmetric=bool(undirected))
 
 

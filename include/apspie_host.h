@@ -33,6 +33,11 @@ void apspie_host_csr_free(apspie_host_csr *g);
  * sorts by (row, col) and drops repeated pairs (self-loops kept), as makeSymmetric does;
  * otherwise rows keep file order. Values are returned as float (val_type F32). */
 apspie_status apspie_load_mtx(const char *path, int undirected, apspie_host_csr *out);
+/* The same loader with the entry lines parsed and the pairs sorted on `threads` host
+ * threads (0 = all); one entry per line assumed, as in every Matrix Market file. Same
+ * result as apspie_load_mtx. No reference counterpart (the reference parses with fscanf on
+ * one thread, src/util.cuh:370-430). */
+apspie_status apspie_load_mtx_threads(const char *path, int undirected, int threads, apspie_host_csr *out);
 
 /* Undirected R-MAT graph: 2^scale vertices, edge_factor * 2^scale generated edges.
  * Edge k (k = 0, 1, ...) takes `scale` draws of std::mt19937(seed) through

@@ -141,3 +141,48 @@ def test_mtx_loader_weighted_and_comments(tmp_path):
     np.testing.assert_array_equal(g.row_ptr, [0, 2, 2, 3])
     np.testing.assert_array_equal(g.col_ind, [1, 2, 0])
     np.testing.assert_allclose(g.val, [0.5, 2.25, 4.0])
+
+
+def _write_mtx(path, m, n, rows, cols, vals=None, comments=("%%MatrixMarket matrix coordinate real general",)):
+    with open(path, "w") as f:
+        for c in comments:
+            f.write(c + "\n")
+        f.write(f"{m} {n} {len(rows)}\n")
+        for k in range(len(rows)):
+            if vals is None:
+                f.write(f"{cols[k] + 1} {rows[k] + 1}\n")
+            else:
+                f.write(f"{cols[k] + 1} {rows[k] + 1} {vals[k]:.6g}\n")
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+@pytest.mark.parametrize("undirected", [False, True])
+def test_parallel_mtx_loader_equals_serial(tmp_path, weighted, undirected):
+    rng = np.random.default_rng(11 + weighted + 2 * undirected)
+    m = 3000
+    ne = 40000
+    rows = rng.integers(0, m, ne)
+    cols = rng.integers(0, m, ne)
+    rows[:500] = cols[:500]  # self-loops
+    rows[500:1500], cols[500:1500] = rows[2000:3000], cols[2000:3000]  # repeated pairs
+    vals = rng.uniform(-2, 2, ne) if weighted else None
+    p = tmp_path / "g.mtx"
+    _write_mtx(p, m, m, rows, cols, vals, comments=("%%MatrixMarket matrix coordinate real general", "% a", "%b"))
+    ref = ap.load_mtx(str(p), undirected)
+    for threads in (1, 2, 7, 0):
+        got = ap.load_mtx(str(p), undirected, threads=threads)
+        assert got.m == ref.m and got.n == ref.n
+        np.testing.assert_array_equal(got.row_ptr, ref.row_ptr)
+        np.testing.assert_array_equal(got.col_ind, ref.col_ind)
+        np.testing.assert_array_equal(got.val, ref.val)
+
+
+def test_parallel_mtx_loader_short_file_and_errors(tmp_path):
+    p = tmp_path / "short.mtx"
+    with open(p, "w") as f:
+        f.write("%%MatrixMarket\n4 4 10\n1 2\n2 3\n")  # fewer entries than promised
+    a, b = ap.load_mtx(str(p), False), ap.load_mtx(str(p), False, threads=3)
+    np.testing.assert_array_equal(a.row_ptr, b.row_ptr)
+    np.testing.assert_array_equal(a.col_ind, b.col_ind)
+    with pytest.raises(ap.ApspieError):
+        ap.load_mtx(str(tmp_path / "missing.mtx"), False, threads=2)
