@@ -30,6 +30,10 @@ constexpr int kTcBlock = 256;
 constexpr int kEmpty = -1;
 constexpr int kTcBins = 4;        // 0 nothing to do | 1 warp | 2 block/shared | 3 block/global
 constexpr int kWarpSet = 512;     // slots (mask <= 256)
+#ifndef APSPIE_TC_CHUNKS
+#define APSPIE_TC_CHUNKS 4
+#endif
+constexpr int kTcChunks = APSPIE_TC_CHUNKS;  // 32-wedge chunks a warp gathers at once
 constexpr int kBlockSet = 4096;   // slots (mask <= 2048)
 
 struct TcInfo {
@@ -278,19 +282,28 @@ __global__ void __launch_bounds__(kTcBlock) tc_warp(const int *__restrict__ task
         // wedges in chunks of 32: the next 32 listed rows' starts that fall inside the
         // chunk are marked in a 32-bit word (distinct, since every listed row is
         // non-empty); each lane's row is o0 plus the marks at or before its position
-        for (int base = w0; base < w1; base += 32) {
-            const int nb = o0 + 1 + lane;
-            const int st = nb <= nv ? sm.soff[nb] - base : 32;
-            const unsigned mark = (st >= 0 && st < 32) ? (1u << st) : 0u;
-            const unsigned starts = __reduce_or_sync(0xffffffffu, mark);
-            const unsigned upto = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
-            const int own = o0 + __popc(starts & upto);
-            const int q = base + lane;
-            if (q < w1) {
-                const int j = __ldg(ci + sm.rs[own] + (q - sm.soff[own]));
-                hits += set_find<false>(sm.keys, kWarpSet, LOG, j) ? 1 : 0;
+        // kTcChunks chunks per step, so that each lane has that many gathers in flight
+        const unsigned upto = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);
+        for (int base = w0; base < w1; base += 32 * kTcChunks) {
+            int own[kTcChunks], q[kTcChunks];
+#pragma unroll
+            for (int h = 0; h < kTcChunks; ++h) {
+                const int cb = base + 32 * h;
+                const int nb = o0 + 1 + lane;
+                const int st = nb <= nv ? sm.soff[nb] - cb : 32;
+                const unsigned mark = (st >= 0 && st < 32) ? (1u << st) : 0u;
+                const unsigned starts = __reduce_or_sync(0xffffffffu, mark);
+                own[h] = o0 + __popc(starts & upto);
+                q[h] = cb + lane;
+                o0 += __popc(starts);
             }
-            o0 += __popc(starts);
+            int j[kTcChunks];
+#pragma unroll
+            for (int h = 0; h < kTcChunks; ++h)
+                j[h] = q[h] < w1 ? __ldg(ci + sm.rs[own[h]] + (q[h] - sm.soff[own[h]])) : -1;
+#pragma unroll
+            for (int h = 0; h < kTcChunks; ++h)
+                if (q[h] < w1) hits += set_find<false>(sm.keys, kWarpSet, LOG, j[h]) ? 1 : 0;
         }
         __syncwarp();
     }
