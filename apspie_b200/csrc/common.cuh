@@ -102,7 +102,7 @@ struct apspie_ctx {
     int spgemm_block_max = 1024;    // SpGEMM shared-table tier: rows of <= this many products
     int tc_task_work = 4096;        // TC wedges per warp task
     int tc_orient = 1;              // TC: re-orient L by degree
-    int sssp_batch_groups = 0;      // batched SSSP: 0 auto, > 0 query groups, < 0 multi-query kernel
+    int sssp_batch_groups = 0;      // batched SSSP: <= 0 multi-query kernel, > 0 query groups
     int use_tuning = 1;             // consult tune_table
     std::vector<apspie_tune_entry> tune_table;
 };
@@ -124,6 +124,8 @@ apspie_status scratch2_reserve(apspie_ctx *ctx, size_t bytes, void **out);
 apspie_status validate_csr(apspie_ctx *ctx, const apspie_csr *A, bool need_square);
 // Checks host-visible CSR view fields (no device access).
 apspie_status check_csr_view(apspie_ctx *ctx, const apspie_csr *A, const char *who);
+// Co-resident blocks a persistent kernel with per_sm blocks per SM may launch on ctx.
+int persistent_cap(const apspie_ctx *ctx, int per_sm);
 // Cooperative launch of a persistent kernel with the largest co-resident grid.
 // `work` (edges the graph holds) sizes the grid: about one block per kWorkPerBlock edges,
 // at least one per SM, at most the co-resident limit (barrier cost grows with blocks).

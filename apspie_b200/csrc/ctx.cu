@@ -134,15 +134,23 @@ apspie_status validate_csr(apspie_ctx *ctx, const apspie_csr *A, bool need_squar
     return APSPIE_OK;
 }
 
+int persistent_cap(const apspie_ctx *ctx, int per_sm) {
+    // a context that shares the device with grid_share - 1 others takes 1/grid_share of the
+    // co-resident capacity, so that all of them fit at once. Whole blocks per SM: then each
+    // kernel holds at most 1/grid_share of every per-SM resource (registers, shared memory,
+    // threads), whichever limits it, and kernels of different footprints still fit together
+    const int share = std::max(1, ctx->grid_share);
+    if (per_sm >= share) return per_sm / share * ctx->num_sms;
+    return std::max(1, per_sm * ctx->num_sms / share);
+}
+
 apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, void **args,
                                 long long work, int *grid_out) {
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, block, 0);
     if (e != cudaSuccess) return cuda_error(ctx, e, "occupancy query");
     if (per_sm < 1) return set_error(ctx, APSPIE_ERR_CUDA, "persistent kernel cannot be resident");
-    // a context that shares the device with grid_share - 1 others takes 1/grid_share of
-    // the co-resident capacity, so that all of them fit at once
-    const int cap = std::max(1, per_sm * ctx->num_sms / std::max(1, ctx->grid_share));
+    const int cap = persistent_cap(ctx, per_sm);
     int grid = cap;
     const long long want = (work + kWorkPerBlock - 1) / kWorkPerBlock;
     if (want < grid) grid = static_cast<int>(want < ctx->num_sms ? ctx->num_sms : want);

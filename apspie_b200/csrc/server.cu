@@ -12,10 +12,14 @@
 //           (6 by default) run apspie_bfs each instead, which is faster for so few;
 //   MIS  -> one apspie_mis (the fixed priorities make every MIS query on a graph the same
 //           question), the set copied to every waiting request;
-//   SSSP -> one apspie_sssp per request written straight into its output by default (the
-//           single-source kernel orders its work by distance band and beats the batched
-//           Bellman-Ford kernel per query), or, with apspie_server_set_sssp_fold(s, n > 1),
-//           apspie_sssp_batch over up to n sources, rows copied likewise.
+//   SSSP -> apspie_sssp_batch over up to sssp_fold sources (max_batch by default), rows
+//           staged and copied into the requests' buffers, when at least sssp_min_batch
+//           requests wait; fewer run apspie_sssp each, straight into their outputs. By
+//           default graphs of at most 2^19 vertices fold from 4 * sqrt(m / 65536)
+//           waiting requests (4 at R-MAT scale 16, 8 at 18: about where one multi-query
+//           launch overtakes as many single-source launches); larger graphs do not fold,
+//           because the multi-query kernel is throughput-bound and a slot holds only its
+//           share of the SMs, while single-source queries spread over all slots.
 // A launch is admitted only if resident graphs + the slots' reserved scratch + the batch's
 // output staging fit the budget; otherwise it waits for a running launch to finish.
 // Requests that arrive while launches run are picked up by the next free slot (no wait for
@@ -23,9 +27,11 @@
 // so it is identical whether the request ran alone or in a mix.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <thread>
@@ -82,8 +88,9 @@ struct apspie_server {
     int device = 0;
     int64_t budget = 0;
     int max_batch = 512;
-    int sssp_fold = 1;  // SSSP requests per launch (1: the single-source kernel)
-    int bfs_min_batch = 6;  // fewer waiting BFS requests run the single-source kernel
+    int sssp_fold = 1 << 30;  // SSSP requests per launch (also capped by max_batch)
+    int bfs_min_batch = 6;     // fewer waiting BFS requests run the single-source kernel
+    int sssp_min_batch = 0;    // fewer waiting SSSP requests run the single-source kernel (0: by size)
     std::vector<apspie::Graph> graphs;
     size_t graph_bytes = 0;
     std::vector<apspie::Slot> slots;
@@ -105,24 +112,34 @@ namespace apspie {
 namespace {
 
 // A launch of n requests of `kind` runs the batched kernel when n reaches the kind's
-// minimum batch (BFS: bfs_min; SSSP: 2; MIS always folds); smaller launches run the
-// single-source kernel once per request, straight into each request's output.
-bool batched(int kind, int n, int bfs_min) {
-    return (kind == APSPIE_QUERY_BFS && n >= bfs_min) || (kind == APSPIE_QUERY_SSSP && n > 1);
+// minimum batch (MIS always folds); smaller launches run the single-source kernel once
+// per request, straight into each request's output.
+struct MinBatch {
+    int bfs, sssp;
+};
+bool batched(int kind, int n, MinBatch mb) {
+    return (kind == APSPIE_QUERY_BFS && n >= mb.bfs) || (kind == APSPIE_QUERY_SSSP && n >= mb.sssp && n > 1);
+}
+MinBatch min_batch(const apspie_server *s, const apspie_csr &g) {
+    int sssp = s->sssp_min_batch;
+    if (sssp <= 0)
+        sssp = g.m > (1 << 19) ? std::numeric_limits<int>::max()
+                               : std::max(2, static_cast<int>(std::lround(4.0 * std::sqrt(g.m / 65536.0))));
+    return {s->bfs_min_batch, sssp};
 }
 
 // Scratch the launch reserves in the slot's arena.
-size_t arena_need(const apspie_csr &g, int kind, int n, int bfs_min) {
+size_t arena_need(const apspie_csr &g, int kind, int n, MinBatch mb) {
     if (kind == APSPIE_QUERY_MIS) return mis_scratch_need(g.m);
-    if (!batched(kind, n, bfs_min)) return traversal_scratch_need(g.m);
+    if (!batched(kind, n, mb)) return traversal_scratch_need(g.m);
     return kind == APSPIE_QUERY_BFS ? bfs_batch_scratch_need(g.m, n) + 8192  // + the row-pointer table
                                     : sssp_batch_scratch_need(g.m, n);
 }
 
 // Batched SSSP launches stage their n rows before copying them out (batched BFS writes
 // straight into the requests' buffers).
-size_t stage_need(const apspie_csr &g, int kind, int n, int bfs_min) {
-    return kind == APSPIE_QUERY_SSSP && batched(kind, n, bfs_min) ? static_cast<size_t>(n) * g.m * 4 : 0;
+size_t stage_need(const apspie_csr &g, int kind, int n, MinBatch mb) {
+    return kind == APSPIE_QUERY_SSSP && batched(kind, n, mb) ? static_cast<size_t>(n) * g.m * 4 : 0;
 }
 
 // Device bytes a slot holds now (its arena never shrinks; staging is kept for reuse).
@@ -133,12 +150,12 @@ size_t slot_held(const Slot &sl) {
 
 // Extra device bytes running (kind, n) on the slot would allocate (arena growth keeps
 // 1/8 headroom, as scratch_reserve does).
-size_t slot_growth(const Slot &sl, const apspie_csr &g, int kind, int n, int bfs_min) {
+size_t slot_growth(const Slot &sl, const apspie_csr &g, int kind, int n, MinBatch mb) {
     const size_t cur = static_cast<size_t>(apspie_ctx_scratch_bytes(sl.ctx));
-    const size_t an = arena_need(g, kind, n, bfs_min);
-    const size_t sn = stage_need(g, kind, n, bfs_min);
+    const size_t an = arena_need(g, kind, n, mb);
+    const size_t sn = stage_need(g, kind, n, mb);
     return (an > cur ? an + an / 8 - cur : 0) + (sn > sl.stage_cap ? sn - sl.stage_cap : 0) +
-           (batched(kind, n, bfs_min) && sl.src_cap < n ? static_cast<size_t>(std::max(n, 512)) * 4 : 0);
+           (batched(kind, n, mb) && sl.src_cap < n ? static_cast<size_t>(std::max(n, 512)) * 4 : 0);
 }
 
 void finish_batch(apspie_server *s, Slot &sl) {
@@ -164,7 +181,7 @@ void launch_batch(apspie_server *s, Slot &sl) {
     const Graph &g = s->graphs[sl.batch.front().graph];
     apspie_status st = APSPIE_OK;
     const int n = static_cast<int>(sl.batch.size());
-    if (sl.kind != APSPIE_QUERY_MIS && !batched(sl.kind, n, s->bfs_min_batch)) {
+    if (sl.kind != APSPIE_QUERY_MIS && !batched(sl.kind, n, min_batch(s, g.view))) {
         for (int i = 0; i < n && st == APSPIE_OK; ++i) {
             const Request &r = sl.batch[i];
             st = sl.kind == APSPIE_QUERY_BFS
@@ -265,11 +282,11 @@ void worker_loop(apspie_server *s) {
             if (kind == APSPIE_QUERY_SSSP) n = std::min(n, s->sssp_fold);
             size_t held = s->graph_bytes;
             for (auto &other : s->slots) held += slot_held(other);
-            size_t need = slot_growth(sl, g.view, kind, n, s->bfs_min_batch);
+            size_t need = slot_growth(sl, g.view, kind, n, min_batch(s, g.view));
             // shrink the batch until its growth fits the budget
             while (n > 1 && held + need > static_cast<size_t>(s->budget)) {
                 n /= 2;
-                need = slot_growth(sl, g.view, kind, n, s->bfs_min_batch);
+                need = slot_growth(sl, g.view, kind, n, min_batch(s, g.view));
             }
             const size_t fixed = held;
             if (held + need > static_cast<size_t>(s->budget)) {
@@ -388,6 +405,12 @@ apspie_status apspie_server_set_bfs_min_batch(apspie_server *s, int32_t min_batc
     return APSPIE_OK;
 }
 
+apspie_status apspie_server_set_sssp_min_batch(apspie_server *s, int32_t min_batch) {
+    if (!s || s->started || min_batch < 0) return APSPIE_ERR_INVALID_ARG;
+    s->sssp_min_batch = min_batch;
+    return APSPIE_OK;
+}
+
 apspie_status apspie_server_start(apspie_server *s) {
     if (!s || s->started) return APSPIE_ERR_INVALID_ARG;
     if (s->graph_bytes + s->slot_reserve * s->slots.size() > static_cast<size_t>(s->budget)) return APSPIE_ERR_OOM;
@@ -401,7 +424,8 @@ apspie_status apspie_server_start(apspie_server *s) {
     if (mmax > 0) {
         full = std::max(full, mis_scratch_need(mmax));
         full = std::max(full, bfs_batch_scratch_need(mmax, s->max_batch) + 8192);
-        if (s->sssp_fold > 1) full = std::max(full, sssp_batch_scratch_need(mmax, s->sssp_fold));
+        const int fold = std::min(s->sssp_fold, s->max_batch);
+        if (fold > 1) full = std::max(full, sssp_batch_scratch_need(mmax, fold));
     }
     const size_t with_headroom = full + full / 8;
     const bool fits = s->graph_bytes + with_headroom * s->slots.size() <= static_cast<size_t>(s->budget);

@@ -1,22 +1,23 @@
 // Batched multi-source SSSP: many sources on one resident graph in ONE persistent launch.
 //
-// By default apspie_sssp_batch runs the query groups of traverse.cu (each group of blocks
-// runs the banded single-source SSSP on its share of the sources). The multi-query kernel
-// below (apspie_ctx_set_sssp_batch_groups(ctx, -1)) reads each frontier row once for
-// all of its queries instead, but relaxes in Bellman-Ford order.
+// By default apspie_sssp_batch runs the multi-query kernel below: it reads each frontier
+// row once for all of its changed queries and relaxes in label-correcting (Bellman-Ford)
+// order. apspie_ctx_set_sssp_batch_groups(ctx, g > 0) runs the query groups of traverse.cu
+// instead (g groups of blocks, each running the banded single-source SSSP on its share of
+// the sources).
 //
-// Frontier entries are (vertex u, query word w) pairs whose "changed" bits (the queries
-// whose distance at u dropped in the previous iteration) are non-zero; an entry's weight
-// is deg(u), so the merge-path expander balances the edges, and every lane relaxes its
-// edge (u, v) for each changed query of the word: nd = dist[q][u] + w(u,v), atomicMin into
-// dist[q][v], and the first bit set in v's next word enqueues the entry (v, w). Every
-// query is the same label-correcting fixed point as apspie_sssp computes alone (exact
-// shortest distances for non-negative integer weights), but the column indices and weights
-// of a frontier row are read once for all of its changed queries, and all queries share
-// the iterations' barriers.
-//
-// Distances are kept as unsigned values in the query-major output out[q * m + v]
-// initialised to 0xFFFFFFFF, which is -1 as int32: unreached vertices need no final pass.
+// Labels are vertex-major: the distances of one vertex for the 32 queries of word w sit in
+// one 128-byte line, lab[(v * W + w) * 32 + q % 32]. Frontier entries are (vertex u, query
+// word w) pairs whose "changed" bits (the queries whose distance at u dropped in the
+// previous iteration) are non-zero; an entry's weight is deg(u), so the merge-path
+// expander balances the edges. Each warp then walks its lanes' edges one at a time with
+// the lanes standing for the word's 32 queries: lane q reads u's and v's labels of query q
+// (two coalesced line reads shared by the whole word), relaxes nd = dist[q][u] + w(u,v) if
+// q changed at u, and atomicMin's the label; a ballot collects the improved queries and the
+// edge's own lane ORs them into v's next changed word, enqueueing (v, w) on the first bit.
+// Every query reaches the same label-correcting fixed point as apspie_sssp computes alone
+// (exact shortest distances for non-negative integer weights). A last pass transposes the
+// labels into the query-major output out[q * m + v] (0xFFFFFFFF, -1 as int32, unreached).
 // Each launch serves at most 32 * W queries with (nnz + m) * W < 2^31 (int32 item counts).
 #include <algorithm>
 #include <cstring>
@@ -26,8 +27,21 @@
 namespace apspie {
 namespace {
 
+#ifndef APSPIE_SB_MINB
+#define APSPIE_SB_MINB 5
+#endif
+#ifndef APSPIE_SB_UNROLL
+#define APSPIE_SB_UNROLL 4
+#endif
+#ifndef APSPIE_SB_VT
+#define APSPIE_SB_VT 2
+#endif
 constexpr int kSbBlock = 256;
-constexpr int kSbVT = 4;
+constexpr int kSbVT = APSPIE_SB_VT;
+constexpr int kSbUnroll = APSPIE_SB_UNROLL;  // edges whose label reads a warp issues together
+// every lane's edge is visited exactly once per pass: a second visit would not record the
+// queries it improves
+static_assert(32 % kSbUnroll == 0, "the unroll must divide the warp");
 using SbSmem = ExpandSmem<kSbBlock, kSbVT>;
 using SbWarp = SbSmem::Warp;
 using SbWQ = WarpQueue<SbSmem::QCAP>;
@@ -40,7 +54,7 @@ struct SbArgs {
     const int *__restrict__ col_ind;
     const int *__restrict__ wt;
     const int *__restrict__ srcs;
-    unsigned *dist;        // nq x m, pre-filled with 0xFFFFFFFF
+    unsigned *lab;         // m x W x 32 labels, vertex-major, pre-filled with 0xFFFFFFFF
     unsigned *chg[2];      // m x W changed-query words (ping-pong)
     unsigned *cbits;       // per frontier entry: its changed word (copied in phase A)
     int *q[2];             // frontier entries u * W + w
@@ -54,7 +68,7 @@ struct RowOfPacked {
     __device__ __forceinline__ int operator()(int e) const { return e / W; }
 };
 
-__global__ void __launch_bounds__(kSbBlock) sssp_batch_kernel(SbArgs a) {
+__global__ void __launch_bounds__(kSbBlock, APSPIE_SB_MINB) sssp_batch_kernel(SbArgs a) {
     __shared__ SbSmem sm;
     timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
@@ -63,6 +77,7 @@ __global__ void __launch_bounds__(kSbBlock) sssp_batch_kernel(SbArgs a) {
     const int m = a.m, W = a.W;
     const long long mw = static_cast<long long>(m) * W;
     const int wid = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
 
     for (long long i = gtid; i < mw; i += gstride) {
         a.chg[0][i] = 0u;
@@ -78,8 +93,8 @@ __global__ void __launch_bounds__(kSbBlock) sssp_batch_kernel(SbArgs a) {
             int e = 0;
             if (qi < a.nq) {
                 const int v = a.srcs[qi];
-                a.dist[static_cast<long long>(qi) * m + v] = 0u;
                 e = v * W + (qi >> 5);
+                a.lab[static_cast<size_t>(e) * 32 + (qi & 31)] = 0u;
                 fresh = atomicOr(a.chg[0] + e, 1u << (qi & 31)) == 0u;
             }
             wq.push(fresh, e);
@@ -119,56 +134,88 @@ __global__ void __launch_bounds__(kSbBlock) sssp_batch_kernel(SbArgs a) {
         SbWQ wq(sm.qbuf[wid][0], qn, &a.ctl->qlen[cur ^ 1]);
         const int *col = a.col_ind;
         const int *wt = a.wt;
-        unsigned *dist = a.dist;
+        unsigned *lab = a.lab;
         TravCtl *ctl = a.ctl;
         int *sticky = a.sticky;
         frontier_expand<kSbBlock, kSbVT, true>(
             nf, E, a.loc_off, a.rs, sm,
             [&](int j, int k, SbWarp &ws) {
                 const int e = __ldcg(qc + j);
-                ws.aux[k] = e / W;           // vertex u
-                ws.flag[k] = e - (e / W) * W;  // query word w
+                ws.aux[k] = e;                  // entry u * W + w
+                ws.flag[k] = e - (e / W) * W;   // query word w
                 ws.aux2[k] = static_cast<int>(__ldcg(cbits + j));
             },
             [&](const bool (&valid)[kSbVT], const int (&kk)[kSbVT], const int (&idx)[kSbVT], SbWarp &ws) {
-                int v[kSbVT], w8[kSbVT];
+                // this lane's edges: target entry (v, w), weight, source entry and its changed bits
+                int tv[kSbVT], we[kSbVT], eu[kSbVT];
+                unsigned bits[kSbVT];
 #pragma unroll
                 for (int r = 0; r < kSbVT; ++r) {
-                    v[r] = valid[r] ? __ldg(col + idx[r]) : 0;
-                    w8[r] = valid[r] ? __ldg(wt + idx[r]) : 0;
+                    tv[r] = eu[r] = 0;
+                    we[r] = 0;
+                    bits[r] = 0u;
+                    if (valid[r]) {
+                        const int v = __ldg(col + idx[r]);
+                        we[r] = __ldg(wt + idx[r]);
+                        eu[r] = ws.aux[kk[r]];
+                        tv[r] = v * W + ws.flag[kk[r]];
+                        bits[r] = static_cast<unsigned>(ws.aux2[kk[r]]);
+                    }
                 }
 #pragma unroll
                 for (int r = 0; r < kSbVT; ++r) {
-                    bool fresh = false;
-                    int ent = 0;
-                    if (valid[r]) {
-                        const int u = ws.aux[kk[r]];
-                        const int w = ws.flag[kk[r]];
-                        unsigned bits = static_cast<unsigned>(ws.aux2[kk[r]]);
-                        if (w8[r] < 0) {
-                            raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSbNeg);
-                            bits = 0u;
+                    const unsigned vmask = __ballot_sync(0xffffffffu, bits[r] != 0u);
+                    if (vmask == 0u) continue;
+                    unsigned mine = 0u;  // improved queries of this lane's edge r
+#pragma unroll 1
+                    for (int l0 = 0; l0 < 32; l0 += kSbUnroll) {
+                        if (((vmask >> l0) & ((1u << kSbUnroll) - 1u)) == 0u) continue;
+                        unsigned du[kSbUnroll], dv[kSbUnroll];
+                        int ev[kSbUnroll], wl[kSbUnroll];
+                        bool act[kSbUnroll];
+#pragma unroll
+                        for (int t = 0; t < kSbUnroll; ++t) {
+                            const int l = l0 + t;
+                            ev[t] = __shfl_sync(0xffffffffu, tv[r], l);
+                            wl[t] = __shfl_sync(0xffffffffu, we[r], l);
+                            const int u = __shfl_sync(0xffffffffu, eu[r], l);
+                            const unsigned b = __shfl_sync(0xffffffffu, bits[r], l);
+                            act[t] = (b >> lane) & 1u;
+                            // coherent reads: a label lowered since the entry was queued must be
+                            // seen (its change bit was consumed in phase A)
+                            du[t] = act[t] ? __ldcg(lab + static_cast<size_t>(u) * 32 + lane) : 0u;
+                            dv[t] = act[t] ? __ldcg(lab + static_cast<size_t>(ev[t]) * 32 + lane) : 0u;
                         }
-                        unsigned newbits = 0u;
-                        while (bits) {
-                            const int b = __ffs(bits) - 1;
-                            bits &= bits - 1;
-                            const long long qo = static_cast<long long>(w * 32 + b) * m;
-                            const unsigned du = __ldcg(dist + qo + u);
-                            const unsigned long long nd = static_cast<unsigned long long>(du) + w8[r];
-                            if (nd >= 0x7fffffffull) {
-                                raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSbOverflow);
-                                continue;
+                        // an improvement over the label just read is reported without waiting
+                        // for the atomic's old value: if another edge lowered the label further
+                        // meanwhile, v's query is only re-expanded once more (same values)
+                        bool imp[kSbUnroll];
+#pragma unroll
+                        for (int t = 0; t < kSbUnroll; ++t) {
+                            imp[t] = false;
+                            if (act[t]) {
+                                if (wl[t] < 0) {
+                                    raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSbNeg);
+                                } else {
+                                    const unsigned long long nd = static_cast<unsigned long long>(du[t]) + wl[t];
+                                    if (nd >= 0x7fffffffull) {
+                                        raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSbOverflow);
+                                    } else if (static_cast<unsigned>(nd) < dv[t]) {
+                                        atomicMin(lab + static_cast<size_t>(ev[t]) * 32 + lane, static_cast<unsigned>(nd));
+                                        imp[t] = true;
+                                    }
+                                }
                             }
-                            const unsigned ndu = static_cast<unsigned>(nd);
-                            if (ndu < dist[qo + v[r]] && ndu < atomicMin(dist + qo + v[r], ndu)) newbits |= 1u << b;
                         }
-                        if (newbits) {
-                            ent = v[r] * W + w;
-                            fresh = atomicOr(cn + ent, newbits) == 0u;
+#pragma unroll
+                        for (int t = 0; t < kSbUnroll; ++t) {
+                            const unsigned nb = __ballot_sync(0xffffffffu, imp[t]);
+                            if (lane == l0 + t) mine = nb;
                         }
                     }
-                    wq.push(fresh, ent);
+                    bool fresh = false;
+                    if (mine) fresh = atomicOr(cn + tv[r], mine) == 0u;
+                    wq.push(fresh, tv[r]);
                 }
             },
             [](int, SbWarp &) {});
@@ -183,13 +230,37 @@ __global__ void __launch_bounds__(kSbBlock) sssp_batch_kernel(SbArgs a) {
     }
 }
 
+// Labels (vertex-major, 32 queries per line) -> query-major rows out[q * m + v], one
+// 32-vertex x 32-query tile at a time through shared memory (both sides coalesced).
+__global__ void __launch_bounds__(256) sb_unpack(const unsigned *__restrict__ lab, int m, int W, int nq,
+                                                 unsigned *out) {
+    __shared__ unsigned t[32][33];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const long long ntiles = static_cast<long long>((m + 31) / 32) * W;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int vb = static_cast<int>(tile / W) * 32;
+        const int w = static_cast<int>(tile % W);
+        for (int i = wid; i < 32; i += 8) {
+            const int v = vb + i;
+            t[i][lane] = v < m ? __ldcs(lab + (static_cast<size_t>(v) * W + w) * 32 + lane) : 0u;
+        }
+        __syncthreads();
+        for (int i = wid; i < 32; i += 8) {
+            const int q = w * 32 + i;
+            if (q < nq && vb + lane < m) out[static_cast<size_t>(q) * m + vb + lane] = t[lane][i];
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 size_t sssp_batch_scratch_need(int m, int nq) {
     const int W = ((nq < 512 ? nq : 512) + 31) / 32;
     const size_t mw = static_cast<size_t>(m) * (W > 0 ? W : 1);
-    const size_t multi = Carver::need({mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, kMaxGrid * 4});
-    // the default grouped form: up to 4 groups
+    const size_t multi =
+        Carver::need({mw * 128, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, kMaxGrid * 4});
+    // the grouped form (groups > 0): at most 4 groups are costed here
     const size_t grouped = sssp_group_scratch_need(m, std::max(1, std::min(nq, 4)));
     return std::max(multi, grouped);
 }
@@ -211,7 +282,7 @@ extern "C" apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A,
     if (num_sources < 0 || (num_sources > 0 && (!d_sources || !d_dists)))
         return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_sssp_batch: bad sources/output");
     if (ctx->validate && (st = validate_csr(ctx, A, true)) != APSPIE_OK) return st;
-    if (ctx->sssp_batch_groups >= 0) return sssp_batch_grouped(ctx, A, d_sources, num_sources, d_dists, stats);
+    if (ctx->sssp_batch_groups > 0) return sssp_batch_grouped(ctx, A, d_sources, num_sources, d_dists, stats);
     const int m = A->m;
     // queries per launch: W words with (nnz + m) * W below 2^31 (int32 item counts)
     long long wmax = 0x7fffffffLL / (static_cast<long long>(A->nnz) + m + 1);
@@ -222,14 +293,15 @@ extern "C" apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A,
     for (int q0 = 0; q0 < num_sources; q0 += per_launch) {
         const int nq = std::min(per_launch, num_sources - q0);
         const int W = (nq + 31) / 32;
-        const size_t mi = static_cast<size_t>(m) + 1;
         const size_t mw = static_cast<size_t>(m) * W;
         void *base;
-        st = scratch_reserve(ctx, Carver::need({mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, kMaxGrid * 4}),
-                             &base);
+        st = scratch_reserve(
+            ctx, Carver::need({mw * 128, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, mw * 4, kMaxGrid * 4}),
+            &base);
         if (st != APSPIE_OK) return st;
         Carver c(base);
         SbArgs a;
+        a.lab = c.take<unsigned>(mw * 32);
         a.chg[0] = c.take<unsigned>(mw);
         a.chg[1] = c.take<unsigned>(mw);
         a.cbits = c.take<unsigned>(mw);
@@ -238,7 +310,6 @@ extern "C" apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A,
         a.rs = c.take<int>(mw);
         a.loc_off = c.take<int>(mw);
         a.chunk_sum = c.take<int>(kMaxGrid);
-        (void)mi;
         a.m = m;
         a.nnz = A->nnz;
         a.nq = nq;
@@ -247,15 +318,19 @@ extern "C" apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A,
         a.col_ind = A->col_ind;
         a.wt = static_cast<const int *>(A->val);
         a.srcs = d_sources + q0;
-        a.dist = reinterpret_cast<unsigned *>(d_dists + static_cast<size_t>(q0) * m);
         a.ctl = ctx->d_ctl;
         a.sticky = ctx->d_sticky_err;
-        cudaError_t e = cudaMemsetAsync(a.dist, 0xff, static_cast<size_t>(nq) * m * sizeof(int32_t), ctx->stream);
+        cudaError_t e = cudaMemsetAsync(a.lab, 0xff, mw * 32 * sizeof(unsigned), ctx->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(TravCtl), ctx->stream);
         if (e != cudaSuccess) return cuda_error(ctx, e, "apspie_sssp_batch reset");
         void *args[] = {&a};
         st = launch_persistent(ctx, reinterpret_cast<const void *>(sssp_batch_kernel), kSbBlock, args, 1LL << 40);
         if (st != APSPIE_OK) return st;
+        const long long tiles = static_cast<long long>((m + 31) / 32) * W;
+        const int ublocks = static_cast<int>(std::min<long long>(tiles, ctx->num_sms * 16LL));
+        sb_unpack<<<ublocks, 256, 0, ctx->stream>>>(
+            a.lab, m, W, nq, reinterpret_cast<unsigned *>(d_dists + static_cast<size_t>(q0) * m));
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_error(ctx, e, "apspie_sssp_batch unpack");
         if (stats) {
             apspie_run_stats part;
             if ((st = finish_call(ctx, &part, "apspie_sssp_batch")) != APSPIE_OK) return st;

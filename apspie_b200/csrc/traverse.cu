@@ -24,6 +24,9 @@ namespace {
 #ifndef APSPIE_SSSP_MINB
 #define APSPIE_SSSP_MINB 4
 #endif
+#ifndef APSPIE_SSSP_RED
+#define APSPIE_SSSP_RED 1
+#endif
 #ifndef APSPIE_SSSP_PREREAD
 #define APSPIE_SSSP_PREREAD 1
 #endif
@@ -580,7 +583,8 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
                 }
                 // plain (L1-cacheable) reads: a stale, larger value only costs an extra atomic
 #pragma unroll
-                for (int r = 0; r < kVT; ++r) cd[r] = (valid[r] && APSPIE_SSSP_PREREAD) ? dist[v[r]] : INF;
+                for (int r = 0; r < kVT; ++r)
+                    cd[r] = (valid[r] && APSPIE_SSSP_PREREAD) ? (APSPIE_SSSP_RED ? __ldcg(dist + v[r]) : dist[v[r]]) : INF;
 #pragma unroll
                 for (int r = 0; r < kVT; ++r) {
                     imp[r] = false;
@@ -606,14 +610,21 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
                         imp[r] = nd[r] < cd[r];
                     }
                 }
-                int old[kVT];
+                bool got[kVT];  // the relaxation lowered v's distance
 #pragma unroll
-                for (int r = 0; r < kVT; ++r) old[r] = imp[r] ? atomicMin(dist + v[r], nd[r]) : 0;
+                for (int r = 0; r < kVT; ++r) {
+                    if (APSPIE_SSSP_RED) {
+                        if (imp[r]) atomicMin(dist + v[r], nd[r]);
+                        got[r] = imp[r];
+                    } else {
+                        got[r] = imp[r] && nd[r] < atomicMin(dist + v[r], nd[r]);
+                    }
+                }
                 bool near[kVT], far[kVT];
 #pragma unroll
                 for (int r = 0; r < kVT; ++r) {
                     near[r] = far[r] = false;
-                    if (imp[r] && nd[r] < old[r]) {
+                    if (got[r]) {
                         const unsigned bit = 1u << (v[r] & 31);
                         const double ndv = is_float ? static_cast<double>(__int_as_float(nd[r]))
                                                     : static_cast<double>(nd[r]);
@@ -631,7 +642,7 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
                     int dg[kVT];
 #pragma unroll
                     for (int r = 0; r < kVT; ++r) {
-                        rec[r] = imp[r] && nd[r] < old[r] &&
+                        rec[r] = got[r] &&
                                  (is_float ? static_cast<double>(__int_as_float(nd[r]))
                                            : static_cast<double>(nd[r])) < T;
                         dg[r] = rec[r] ? __ldg(rp + v[r] + 1) - __ldg(rp + v[r]) : 0;
@@ -1154,7 +1165,7 @@ apspie_status sssp_batch_grouped(apspie_ctx *ctx, const apspie_csr *A, const int
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
         &per_sm, reinterpret_cast<const void *>(sssp_group_kernel), kBlock, 0);
     if (e != cudaSuccess || per_sm < 1) return cuda_error(ctx, e, "occupancy query");
-    const int cap = std::max(1, per_sm * ctx->num_sms / std::max(1, ctx->grid_share));
+    const int cap = persistent_cap(ctx, per_sm);
     const int groups = std::min(sssp_group_count(ctx, nq), cap);
     const int bpg = std::min(cap / groups, kMaxGrid);
     void *base;

@@ -237,7 +237,7 @@ class Context:
         self._check(L.lib().apspie_ctx_set_sssp_band(self.handle, edges), "set_sssp_band")
 
     def set_sssp_batch_groups(self, groups: int) -> None:
-        """Batched SSSP: 0 = 4 query groups, > 0 = that many, < 0 = the multi-query kernel."""
+        """Batched SSSP: <= 0 = the multi-query kernel (default), > 0 = that many query groups."""
         self._check(L.lib().apspie_ctx_set_sssp_batch_groups(self.handle, groups), "set_sssp_batch_groups")
 
     # ---- autotuner
@@ -572,6 +572,9 @@ class Server:
 
     def set_sssp_fold(self, n: int) -> None:
         L.check(L.lib().apspie_server_set_sssp_fold(self.handle, n), None, "server_set_sssp_fold")
+
+    def set_sssp_min_batch(self, n: int) -> None:
+        L.check(L.lib().apspie_server_set_sssp_min_batch(self.handle, n), None, "server_set_sssp_min_batch")
 
     def start(self) -> None:
         L.check(L.lib().apspie_server_start(self.handle), None, "server_start")

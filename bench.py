@@ -515,8 +515,9 @@ def extras_spgemm_tc(ctx, args, ws, local):
 
 
 def extras_batched(ctx, args, ws, local, g):
-    """Batched BFS on R-MAT scale 22 (seed 1): batches of 32/128/512 LCC sources (seed 6)
-    against the plain path looping one source at a time over the same sources."""
+    """Batched BFS and SSSP on R-MAT scale 22 (seed 1, int32 weights from seed 3): batches
+    of 32/128/512 LCC sources (seed 6) against the plain path looping one source at a time
+    over the same sources."""
     import torch
 
     import apspie_b200 as ap
@@ -542,6 +543,26 @@ def extras_batched(ctx, args, ws, local, g):
         res[f"batched_bfs_rmat22_B{nq}"] = {"ms_per_batch": ms, "queries_per_s": ws * nq * 1e3 / ms,
                                             "x_plain": plain_ms * nq / ms, "p99_ms": float(np.percentile(per, 99)),
                                             "exact_checked_rows": bool(exact)}
+        del out
+    # SSSP: the plain loop over 16 sources (each query takes milliseconds), then the batches
+    for x in srcs[:2]:
+        ctx.sssp_into(dg, int(x), one)
+    tot, _ = time_steps(ctx.stream, lambda: [ctx.sssp_into(dg, int(x), one) for x in srcs[:16]], 1)
+    plain_ms = max_over_ranks(ws, tot / 16)
+    res["plain_sssp_rmat22"] = {"ms_per_query": plain_ms, "queries_per_s": ws * 1e3 / plain_ms}
+    for nq in (32, 128, 512):
+        s = torch.from_numpy(srcs[:nq]).to(dev)
+        out = torch.empty((nq, g.m), dtype=torch.int32, device=dev)
+        ctx.sssp_batch_into(dg, s, out)
+        reps = 3 if nq < 512 else 1
+        tot, per = time_steps(ctx.stream, lambda: ctx.sssp_batch_into(dg, s, out), reps)
+        ms = max_over_ranks(ws, tot / reps)
+        # row 0 against the oracle, the last row against the single-source kernel
+        ctx.sssp_into(dg, int(srcs[nq - 1]), one)
+        exact = np.array_equal(out[0].cpu().numpy(), oracle.sssp(g.row_ptr, g.col_ind, g.val, int(srcs[0]))) \
+            and torch.equal(out[nq - 1], one)
+        res[f"batched_sssp_rmat22_B{nq}"] = {"ms_per_batch": ms, "queries_per_s": ws * nq * 1e3 / ms,
+                                             "x_plain": plain_ms * nq / ms, "exact_checked_rows": bool(exact)}
         del out
     return res
 

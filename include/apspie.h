@@ -115,8 +115,8 @@ apspie_status apspie_ctx_set_sssp_delta(apspie_ctx *ctx, int32_t delta);
  * from a degree-weighted distance histogram gathered on the device. edges == 0 (default):
  * nnz / 8 clamped to [2^18, 2^23]; edges < 0: off (expand the whole frontier). */
 apspie_status apspie_ctx_set_sssp_band(apspie_ctx *ctx, int64_t edges);
-/* Batched SSSP: query groups per launch (0 = 4, > 0 = that many, < 0 = the multi-query
- * kernel instead of groups). */
+/* Batched SSSP: <= 0 = the multi-query kernel (default); > 0 = that many query groups,
+ * each running the single-source kernel on its share of the sources. */
 apspie_status apspie_ctx_set_sssp_batch_groups(apspie_ctx *ctx, int32_t groups);
 /* Batched BFS direction switch: a level expands top-down while (active vertices x mean
  * degree) < frac * nnz, else bottom-up (default 0.05; bottom-up only on symmetric graphs). */
@@ -224,11 +224,11 @@ apspie_status apspie_bfs_batch(apspie_ctx *ctx, const apspie_csr *A, const int32
 
 /* Batched multi-source SSSP over int32 weights in one persistent launch. d_dists is
  * num_sources x m int32, query-major (row q = what apspie_sssp returns for d_sources[q]);
- * -1 unreached. By default the launch's blocks split into query groups (4, or
- * apspie_ctx_set_sssp_batch_groups), each running the single-source kernel on its share of
- * the sources side by side with the others. With groups < 0 a multi-query kernel relaxes
- * all queries of a frontier row together instead (32*W queries per launch with
- * (nnz + m) * W < 2^31, W <= 16). */
+ * -1 unreached. By default a multi-query kernel relaxes all changed queries of a frontier
+ * row together, one warp per edge with a lane per query over vertex-major labels
+ * (32*W queries per launch with (nnz + m) * W < 2^31, W <= 16; device scratch about
+ * 160 * m * W bytes). With apspie_ctx_set_sssp_batch_groups(ctx, g > 0) the launch's blocks
+ * split into g query groups instead, each running the single-source kernel on its share. */
 apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources,
                                 int32_t num_sources, int32_t *d_dists, apspie_run_stats *stats);
 

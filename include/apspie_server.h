@@ -51,13 +51,19 @@ apspie_status apspie_server_create(int device, int64_t memory_budget_bytes, int3
  * undirected. MIS priorities are mt19937(mis_seed) outputs per vertex. Before start only. */
 apspie_status apspie_server_add_graph(apspie_server *s, const apspie_host_csr *g, int32_t symmetric,
                                       uint32_t mis_seed, int32_t *graph_id);
-/* SSSP requests folded into one launch (before start; default 1: each request runs the
- * single-source kernel, which orders its work by distance band and is faster per query
- * than the batched kernel on R-MAT graphs; n > 1 folds up to n into apspie_sssp_batch). */
+/* At most max_fold SSSP requests per launch (before start; default max_batch; 1 = every
+ * request runs the single-source kernel). */
 apspie_status apspie_server_set_sssp_fold(apspie_server *s, int32_t max_fold);
 /* BFS requests run the batched kernel only when at least min_batch of them wait on the
  * same graph (before start; default 6); fewer run apspie_bfs each. */
 apspie_status apspie_server_set_bfs_min_batch(apspie_server *s, int32_t min_batch);
+/* SSSP requests run apspie_sssp_batch only when at least min_batch of them wait on the
+ * same graph (before start); fewer run apspie_sssp each. 0 (default) = by graph size:
+ * graphs of at most 2^19 vertices from 4 * sqrt(m / 65536) waiting requests (about where
+ * one multi-query launch overtakes as many single-source launches on R-MAT graphs: 4 at
+ * scale 16, 8 at scale 18), larger graphs never (a slot's multi-query launch holds only
+ * its share of the SMs, while single-source queries spread over all slots). */
+apspie_status apspie_server_set_sssp_min_batch(apspie_server *s, int32_t min_batch);
 /* Reserves the slots' scratch and starts the worker thread. */
 apspie_status apspie_server_start(apspie_server *s);
 /* Queues a request; the answer is written to d_out (device memory of the server's GPU),

@@ -32,14 +32,16 @@ def _out(g, kind):
     return torch.empty(g.m, dtype=torch.uint8 if kind == L.QUERY_MIS else torch.int32, device="cuda")
 
 
-@pytest.mark.parametrize("sssp_fold,bfs_min", [(1, 6), (64, 1), (1, 1000)])
-def test_server_mix_matches_plain_path_alone_and_in_mix(ctx, graphs, sssp_fold, bfs_min):
-    """sssp_fold 1: each SSSP request runs the single-source kernel; 64: SSSP requests are
-    folded into the batched kernel like BFS requests. bfs_min 1: every BFS launch uses the
-    batched kernel; 1000: none does."""
+@pytest.mark.parametrize("sssp_fold,sssp_min,bfs_min", [(1, 0, 6), (64, 2, 1), (512, 0, 1000)])
+def test_server_mix_matches_plain_path_alone_and_in_mix(ctx, graphs, sssp_fold, sssp_min, bfs_min):
+    """sssp_fold 1: each SSSP request runs the single-source kernel; 64 with sssp_min 2:
+    SSSP requests are folded into the batched kernel whenever two or more wait; 512 with
+    0: the defaults (minimum by graph size). bfs_min 1: every BFS launch uses the batched
+    kernel; 1000: none does."""
     srv = ap.Server(0, budget_bytes=8 << 30, slots=2, max_batch=512)
     gids = [srv.add_graph(g) for g in graphs]
     srv.set_sssp_fold(sssp_fold)
+    srv.set_sssp_min_batch(sssp_min)
     srv.set_bfs_min_batch(bfs_min)
     srv.start()
     rng = np.random.default_rng(7)
