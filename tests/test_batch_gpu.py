@@ -99,8 +99,8 @@ def test_batch_rmat22_full_size(ctx):
 @pytest.mark.parametrize("groups", [0, 3, 64, -1])
 @pytest.mark.parametrize("nq", [1, 7, 32, 100, 512])
 def test_sssp_batch_rows_equal_single_sssp(ctx, rmat14, nq, groups):
-    """groups 0: the default 4 query groups; 3 / 64: that many (64 > 7 queries leaves
-    groups idle); -1: the multi-query kernel."""
+    """groups 0 (the default) and -1: the multi-query kernel; 3 / 64: that many query
+    groups (64 > 7 queries leaves groups idle)."""
     g, dg = rmat14
     s = _srcs(g, nq, 4)
     ctx.set_sssp_batch_groups(groups)
@@ -143,3 +143,55 @@ def test_sssp_batch_rmat20_full_size(ctx):
     out = ctx.sssp_batch(dg, s)
     for q in (0, 17, 63):
         np.testing.assert_array_equal(out[q].cpu().numpy(), oracle.sssp(g.row_ptr, g.col_ind, g.val, int(s[q])))
+
+
+def _chain(weights):
+    """Undirected path 0 - 1 - ... - k with the given edge weights."""
+    k = len(weights)
+    rows = [[] for _ in range(k + 1)]
+    for i, w in enumerate(weights):
+        rows[i].append((i + 1, w))
+        rows[i + 1].append((i, w))
+    rp = np.zeros(k + 2, dtype=np.int32)
+    ci, wt = [], []
+    for i, r in enumerate(sorted(x) for x in rows):
+        for c, w in r:
+            ci.append(c)
+            wt.append(w)
+        rp[i + 1] = len(ci)
+    return ap.HostGraph(k + 1, k + 1, rp, np.array(ci, dtype=np.int32), np.array(wt, dtype=np.int32), True)
+
+
+@pytest.mark.parametrize("groups", [0, 2])
+@pytest.mark.parametrize("weights,what", [([5, -3, 2], "negative"), ([1 << 30, 1 << 30, 1], "overflow")])
+def test_sssp_batch_bad_weights_reported_and_context_reusable(ctx, weights, what, groups):
+    """A negative weight, or a distance that leaves int32, is reported as an error (never
+    a hang or a wrong answer), and the context answers the next call correctly."""
+    import torch
+
+    g = _chain(weights)
+    dg = ap.DeviceGraph(g)
+    srcs = torch.tensor([0, 3, 1], dtype=torch.int32, device="cuda")
+    out = torch.empty((3, g.m), dtype=torch.int32, device="cuda")
+    ctx.set_sssp_batch_groups(groups)
+    try:
+        with pytest.raises(ap.ApspieError):
+            ctx.sssp_batch_into(dg, srcs, out, stats=True)
+        good = _chain([5, 3, 2])
+        got = ctx.sssp_batch(ap.DeviceGraph(good), srcs).cpu().numpy()
+    finally:
+        ctx.set_sssp_batch_groups(0)
+    for q, s in enumerate([0, 3, 1]):
+        np.testing.assert_array_equal(got[q], oracle.sssp(good.row_ptr, good.col_ind, good.val, s))
+
+
+def test_sssp_single_source_overflow_reported(ctx):
+    import torch
+
+    g = _chain([1 << 30, 1 << 30, 1])
+    out = torch.empty(g.m, dtype=torch.int32, device="cuda")
+    with pytest.raises(ap.ApspieError):
+        ctx.sssp_into(ap.DeviceGraph(g), 0, out, stats=True)
+    g2 = _chain([(1 << 30) - 1, (1 << 30) - 1])  # 2^31 - 2 is the largest distance allowed
+    np.testing.assert_array_equal(ctx.sssp(ap.DeviceGraph(g2), 0).cpu().numpy(),
+                                  oracle.sssp(g2.row_ptr, g2.col_ind, g2.val, 0))
