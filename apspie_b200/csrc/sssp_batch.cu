@@ -160,8 +160,13 @@ __global__ void __launch_bounds__(kSbBlock, APSPIE_SB_MINB) sssp_batch_kernel(Sb
                         eu[r] = ws.aux[kk[r]];
                         tv[r] = v * W + ws.flag[kk[r]];
                         bits[r] = static_cast<unsigned>(ws.aux2[kk[r]]);
+                        if (we[r] < 0) {  // reported once here; the edge is then left out
+                            raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSbNeg);
+                            bits[r] = 0u;
+                        }
                     }
                 }
+                unsigned *lab_l = lab + lane;  // this lane's query in every label line
 #pragma unroll
                 for (int r = 0; r < kSbVT; ++r) {
                     const unsigned vmask = __ballot_sync(0xffffffffu, bits[r] != 0u);
@@ -183,8 +188,8 @@ __global__ void __launch_bounds__(kSbBlock, APSPIE_SB_MINB) sssp_batch_kernel(Sb
                             act[t] = (b >> lane) & 1u;
                             // coherent reads: a label lowered since the entry was queued must be
                             // seen (its change bit was consumed in phase A)
-                            du[t] = act[t] ? __ldcg(lab + static_cast<size_t>(u) * 32 + lane) : 0u;
-                            dv[t] = act[t] ? __ldcg(lab + static_cast<size_t>(ev[t]) * 32 + lane) : 0u;
+                            du[t] = act[t] ? __ldcg(lab_l + static_cast<size_t>(u) * 32) : 0u;
+                            dv[t] = act[t] ? __ldcg(lab_l + static_cast<size_t>(ev[t]) * 32) : 0u;
                         }
                         // an improvement over the label just read is reported without waiting
                         // for the atomic's old value: if another edge lowered the label further
@@ -193,17 +198,15 @@ __global__ void __launch_bounds__(kSbBlock, APSPIE_SB_MINB) sssp_batch_kernel(Sb
 #pragma unroll
                         for (int t = 0; t < kSbUnroll; ++t) {
                             imp[t] = false;
+                            // an active label is finite (< 2^31 - 1) and the weight is
+                            // non-negative, so the 32-bit sum cannot wrap
+                            const unsigned nd = du[t] + static_cast<unsigned>(wl[t]);
                             if (act[t]) {
-                                if (wl[t] < 0) {
-                                    raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSbNeg);
-                                } else {
-                                    const unsigned long long nd = static_cast<unsigned long long>(du[t]) + wl[t];
-                                    if (nd >= 0x7fffffffull) {
-                                        raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSbOverflow);
-                                    } else if (static_cast<unsigned>(nd) < dv[t]) {
-                                        atomicMin(lab + static_cast<size_t>(ev[t]) * 32 + lane, static_cast<unsigned>(nd));
-                                        imp[t] = true;
-                                    }
+                                if (nd >= 0x7fffffffu) {
+                                    raise_error(ctl, sticky, APSPIE_ERR_INVALID_ARG, kSiteSbOverflow);
+                                } else if (nd < dv[t]) {
+                                    atomicMin(lab_l + static_cast<size_t>(ev[t]) * 32, nd);
+                                    imp[t] = true;
                                 }
                             }
                         }
