@@ -32,7 +32,7 @@ using MsSmem = ExpandSmem<kMsBlock, kMsVT>;
 using MsWarp = MsSmem::Warp;
 using MsWQ = WarpQueue<MsSmem::QCAP>;
 
-enum : int { kSiteMs = 400 };
+enum : int { kSiteMs = 400, kSiteMsBadSource = 450 };
 constexpr int kHeavyDeg = 128;  // pull: rows longer than this are scanned by a whole block
 
 struct MsArgs {
@@ -115,12 +115,17 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
             int v = 0;
             if (qi < a.nq) {
                 v = a.srcs[qi];
-                const unsigned bit = 1u << (qi & 31);
-                atomicOr(a.vis + static_cast<long long>(v) * W + (qi >> 5), bit);
-                atomicOr(a.fr[0] + static_cast<long long>(v) * W + (qi >> 5), bit);
-                depth_row(a, qi)[v] = 0;
-                const unsigned tb = 1u << (v & 31);
-                first = !(atomicOr(a.touched + (v >> 5), tb) & tb);
+                if (v < 0 || v >= a.m) {  // reported; the barrier below then ends the launch
+                    raise_error(a.ctl, a.sticky, APSPIE_ERR_INVALID_ARG, kSiteMsBadSource);
+                    v = 0;
+                } else {
+                    const unsigned bit = 1u << (qi & 31);
+                    atomicOr(a.vis + static_cast<long long>(v) * W + (qi >> 5), bit);
+                    atomicOr(a.fr[0] + static_cast<long long>(v) * W + (qi >> 5), bit);
+                    depth_row(a, qi)[v] = 0;
+                    const unsigned tb = 1u << (v & 31);
+                    first = !(atomicOr(a.touched + (v >> 5), tb) & tb);
+                }
             }
             wq.push(first, v);
         }

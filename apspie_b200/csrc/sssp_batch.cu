@@ -46,7 +46,7 @@ using SbSmem = ExpandSmem<kSbBlock, kSbVT>;
 using SbWarp = SbSmem::Warp;
 using SbWQ = WarpQueue<SbSmem::QCAP>;
 
-enum : int { kSiteSb = 500, kSiteSbNeg = 501, kSiteSbOverflow = 502, kSiteSbCap = 503 };
+enum : int { kSiteSb = 500, kSiteSbNeg = 501, kSiteSbOverflow = 502, kSiteSbCap = 503, kSiteSbBadSource = 504 };
 
 struct SbArgs {
     int m, nnz, nq, W;
@@ -93,9 +93,13 @@ __global__ void __launch_bounds__(kSbBlock, APSPIE_SB_MINB) sssp_batch_kernel(Sb
             int e = 0;
             if (qi < a.nq) {
                 const int v = a.srcs[qi];
-                e = v * W + (qi >> 5);
-                a.lab[static_cast<size_t>(e) * 32 + (qi & 31)] = 0u;
-                fresh = atomicOr(a.chg[0] + e, 1u << (qi & 31)) == 0u;
+                if (v < 0 || v >= m) {  // reported; the barrier below then ends the launch
+                    raise_error(a.ctl, a.sticky, APSPIE_ERR_INVALID_ARG, kSiteSbBadSource);
+                } else {
+                    e = v * W + (qi >> 5);
+                    a.lab[static_cast<size_t>(e) * 32 + (qi & 31)] = 0u;
+                    fresh = atomicOr(a.chg[0] + e, 1u << (qi & 31)) == 0u;
+                }
             }
             wq.push(fresh, e);
         }

@@ -63,6 +63,7 @@ enum : int {
     kSiteSsspBarF0 = 212,
     kSiteSsspBarF1 = 213,
     kSiteSsspGroup = 214,  // and 215
+    kSiteSsspBadSource = 216,
     kSiteMis = 300,
     kSiteMisRoundCap = 301,
 };
@@ -755,6 +756,11 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_group_kernel(Ss
     const int tid = vg.id * kBlock + static_cast<int>(threadIdx.x);
     for (int q = grp; q < g.nq; q += g.groups) {
         a.src = __ldg(g.srcs + q);
+        if (a.src < 0 || a.src >= g.m) {
+            // every block of the group reads the same source and skips the query alike
+            if (tid == 0) raise_error(g.main, a.sticky, APSPIE_ERR_INVALID_ARG, kSiteSsspBadSource);
+            continue;
+        }
         a.dist = g.out + static_cast<size_t>(q) * g.m;
         sssp_body(a, vg);
         // every block of the group is done with the control block before it is reset

@@ -195,3 +195,31 @@ def test_sssp_single_source_overflow_reported(ctx):
     g2 = _chain([(1 << 30) - 1, (1 << 30) - 1])  # 2^31 - 2 is the largest distance allowed
     np.testing.assert_array_equal(ctx.sssp(ap.DeviceGraph(g2), 0).cpu().numpy(),
                                   oracle.sssp(g2.row_ptr, g2.col_ind, g2.val, 0))
+
+
+@pytest.mark.parametrize("kind,groups", [("bfs", 0), ("sssp", 0), ("sssp", 2)])
+@pytest.mark.parametrize("bad", [-1, "m"])
+def test_batch_source_out_of_range_reported(ctx, rmat14, kind, groups, bad):
+    """Sources live in device memory, so the kernels range-check them: an out-of-range
+    source is reported as an invalid argument (nothing is written for it) and the context
+    answers the next call."""
+    import torch
+
+    g, dg = rmat14
+    b = g.m if bad == "m" else bad
+    srcs = torch.tensor([0, b, 5], dtype=torch.int32, device="cuda")
+    out = torch.empty((3, g.m), dtype=torch.int32, device="cuda")
+    ctx.set_sssp_batch_groups(groups)
+    try:
+        with pytest.raises(ap.ApspieError):
+            if kind == "bfs":
+                ctx.bfs_batch_into(dg, srcs, out, stats=True)
+            else:
+                ctx.sssp_batch_into(dg, srcs, out, stats=True)
+        good = torch.tensor([0, 5], dtype=torch.int32, device="cuda")
+        got = (ctx.bfs_batch(dg, good) if kind == "bfs" else ctx.sssp_batch(dg, good)).cpu().numpy()
+    finally:
+        ctx.set_sssp_batch_groups(0)
+    for q, s in enumerate([0, 5]):
+        ref = oracle.bfs(g.row_ptr, g.col_ind, s) if kind == "bfs" else oracle.sssp(g.row_ptr, g.col_ind, g.val, s)
+        np.testing.assert_array_equal(got[q], ref)
