@@ -342,10 +342,10 @@ apspie_status apspie_server_create(int device, int64_t memory_budget_bytes, int3
         }
         sl.ctx->stream = sl.stream;
         // Concurrent persistent grids should all fit on the device at once: each slot's
-        // grids take 1/num_slots of their kernel's co-resident capacity, so the slots'
-        // grids together use at most one device's worth of every SM resource. (A grid
-        // whose blocks could not all be resident would end its wait at a grid barrier with
-        // APSPIE_ERR_TIMEOUT, not hang.)
+        // grids take floor(per-SM occupancy / num_slots) blocks per SM, so every grid holds
+        // at most 1/num_slots of each SM resource and the slots' grids together fit even
+        // when their kernels differ in footprint. (A grid whose blocks could not all be
+        // resident would end its wait at a grid barrier with APSPIE_ERR_TIMEOUT, not hang.)
         sl.ctx->grid_share = num_slots;
     }
     *out = s;
