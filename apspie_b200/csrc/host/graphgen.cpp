@@ -2,11 +2,13 @@
 #include <omp.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "../../../include/apspie_host.h"
@@ -55,51 +57,199 @@ void radix_sort_pairs(std::vector<uint64_t> &key, std::vector<int32_t> &pay, int
     }
 }
 
-// Builds a symmetric CSR from unique canonical pairs (lo < hi) given in ascending
-// (lo, hi) order: row r gets its lower neighbours first (pairs (lo, r), ascending lo),
-// then its upper neighbours (pairs (r, hi), ascending hi) -- sorted rows without a sort.
+// Builds a symmetric CSR from unique canonical pairs (lo << 32 | hi, lo < hi) given in
+// ascending (lo, hi) order: row r gets its lower neighbours first (pairs (lo, r), ascending
+// lo), then its upper neighbours (pairs (r, hi), ascending hi) -- sorted rows without a
+// sort. Threads take contiguous ranges of pairs; per-thread counts of each row's lower
+// neighbours give every thread its own write offsets, so the rows come out in pair order
+// exactly as a single pass would write them.
 void build_symmetric(int m, const std::vector<uint64_t> &pairs, const std::vector<int32_t> *w,
                      apspie_host_csr *out) {
-    const size_t np = pairs.size();
+    const int64_t np = static_cast<int64_t>(pairs.size());
     out->m = out->n = m;
     out->nnz = static_cast<int32_t>(2 * np);
     out->row_ptr = host_alloc<int32_t>(static_cast<size_t>(m) + 1);
-    out->col_ind = host_alloc<int32_t>(2 * np);
+    out->col_ind = host_alloc<int32_t>(static_cast<size_t>(2 * np));
     int32_t *wv = nullptr;
     if (w) {
-        wv = host_alloc<int32_t>(2 * np);
+        wv = host_alloc<int32_t>(static_cast<size_t>(2 * np));
         out->val = wv;
         out->val_type = APSPIE_VAL_I32;
     } else {
         out->val = nullptr;
         out->val_type = APSPIE_VAL_NONE;
     }
-    std::vector<int64_t> deg(static_cast<size_t>(m) + 1, 0);
-    for (size_t i = 0; i < np; ++i) {
-        ++deg[pairs[i] >> 32];
-        ++deg[pairs[i] & 0xffffffffu];
+    // per-thread count arrays: at most about 512 MB of them
+    const int T = std::max(1, std::min<int>(omp_get_max_threads(),
+                                            static_cast<int>((int64_t(1) << 27) / std::max(m, 1))));
+    std::vector<int32_t> low(static_cast<size_t>(T) * m, 0);  // lower-neighbour counts, then offsets
+    std::vector<int64_t> up(static_cast<size_t>(m), 0);       // first pair of row r's upper run
+    std::vector<int32_t> nup(static_cast<size_t>(m), 0);      // length of that run
+    auto lo_of = [&](int64_t i) { return static_cast<int32_t>(pairs[i] >> 32); };
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num();
+        const int64_t i0 = np * t / T, i1 = np * (t + 1) / T;
+        int32_t *h = &low[static_cast<size_t>(t) * m];
+        for (int64_t i = i0; i < i1; ++i) {
+            ++h[static_cast<int32_t>(pairs[i] & 0xffffffffu)];
+            const int32_t lo = lo_of(i);
+            if (i == 0 || lo_of(i - 1) != lo) {  // a run of pairs (lo, *) starts here
+                int64_t j = i + 1;
+                while (j < np && lo_of(j) == lo) ++j;
+                up[lo] = i;
+                nup[lo] = static_cast<int32_t>(j - i);
+            }
+        }
     }
     int64_t run = 0;
     for (int r = 0; r < m; ++r) {
         out->row_ptr[r] = static_cast<int32_t>(run);
-        run += deg[r];
+        for (int t = 0; t < T; ++t) {
+            int32_t &c = low[static_cast<size_t>(t) * m + r];
+            const int32_t n = c;
+            c = static_cast<int32_t>(run);
+            run += n;
+        }
+        up[r] = run - up[r];  // pair i of row r's upper run lands at up[r] + i
+        run += nup[r];
     }
     out->row_ptr[m] = static_cast<int32_t>(run);
-    std::vector<int64_t> cur(out->row_ptr, out->row_ptr + m);
-    for (size_t i = 0; i < np; ++i) {  // lower neighbours
-        const int32_t lo = static_cast<int32_t>(pairs[i] >> 32);
-        const int32_t hi = static_cast<int32_t>(pairs[i] & 0xffffffffu);
-        const int64_t p = cur[hi]++;
-        out->col_ind[p] = lo;
-        if (wv) wv[p] = (*w)[i];
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num();
+        const int64_t i0 = np * t / T, i1 = np * (t + 1) / T;
+        int32_t *h = &low[static_cast<size_t>(t) * m];
+        for (int64_t i = i0; i < i1; ++i) {
+            const int32_t lo = lo_of(i);
+            const int32_t hi = static_cast<int32_t>(pairs[i] & 0xffffffffu);
+            const int64_t p = h[hi]++;  // lower neighbour lo of row hi
+            const int64_t q = up[lo] + i;  // upper neighbour hi of row lo
+            out->col_ind[p] = lo;
+            out->col_ind[q] = hi;
+            if (wv) wv[p] = wv[q] = (*w)[i];
+        }
     }
-    for (size_t i = 0; i < np; ++i) {  // upper neighbours
-        const int32_t lo = static_cast<int32_t>(pairs[i] >> 32);
-        const int32_t hi = static_cast<int32_t>(pairs[i] & 0xffffffffu);
-        const int64_t p = cur[lo]++;
-        out->col_ind[p] = hi;
-        if (wv) wv[p] = (*w)[i];
+}
+
+// MT19937 (Matsumoto and Nishimura, ACM TOMACS 8(1), 1998), the generator std::mt19937
+// implements, advanced one whole 624-word state block per call. The untempered block is
+// handed out; mt_temper turns its words into the generator's outputs, in order.
+class MtBlocks {
+  public:
+    static constexpr int kN = 624, kM = 397;
+    explicit MtBlocks(uint32_t seed) {
+        s_[0] = seed;
+        for (int i = 1; i < kN; ++i) s_[i] = 1812433253u * (s_[i - 1] ^ (s_[i - 1] >> 30)) + static_cast<uint32_t>(i);
     }
+    const uint32_t *next_block() {
+        for (int i = 0; i < kN - kM; ++i) s_[i] = step(s_[i], s_[i + 1], s_[i + kM]);
+        for (int i = kN - kM; i < kN - 1; ++i) s_[i] = step(s_[i], s_[i + 1], s_[i + kM - kN]);
+        s_[kN - 1] = step(s_[kN - 1], s_[0], s_[kM - 1]);
+        return s_;
+    }
+
+  private:
+    static uint32_t step(uint32_t cur, uint32_t nxt, uint32_t far) {
+        const uint32_t y = (cur & 0x80000000u) | (nxt & 0x7fffffffu);
+        return far ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+    }
+    uint32_t s_[kN];
+};
+
+inline uint32_t mt_temper(uint32_t y) {
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    return y ^ (y >> 18);
+}
+
+// Replays recorded untempered MT19937 words as the generator's outputs, so that a standard
+// distribution draws from it exactly what it would draw from std::mt19937 itself.
+struct MtReplay {
+    using result_type = std::mt19937::result_type;
+    const uint32_t *p;
+    static constexpr result_type min() { return std::mt19937::min(); }
+    static constexpr result_type max() { return std::mt19937::max(); }
+    result_type operator()() { return mt_temper(*p++); }
+};
+
+// The R-MAT edge stream of std::mt19937(seed): edge k takes `scale` uniform doubles
+// (std::uniform_real_distribution<double>(0, 1), two generator words each), one per bit
+// level, u's bit then v's from the same draw. One thread advances the generator and
+// copies its words into a ring of chunks; the other threads turn chunks into edges and
+// call edge(k, u, v) for every edge of their chunk. The result is the serial stream's,
+// edge for edge, whatever the thread count.
+template <class Edge>
+void rmat_edges(int scale, int64_t ne, uint32_t seed, double a, double b, double c, Edge edge) {
+    const double ab = a + b, abc = a + b + c;
+    const int64_t per_edge = 2LL * scale;  // generator words per edge
+    const int64_t kChunk = 1 << 14;        // edges per chunk
+    const int64_t nch = (ne + kChunk - 1) / kChunk;
+    auto decode = [&](int64_t k0, int64_t k1, const uint32_t *words) {
+        MtReplay g{words};
+        std::uniform_real_distribution<double> U(0.0, 1.0);
+        for (int64_t k = k0; k < k1; ++k) {
+            uint32_t u = 0, v = 0;
+            for (int l = 0; l < scale; ++l) {
+                const double r = U(g);
+                u = (u << 1) | ((r >= ab) ? 1u : 0u);
+                v = (v << 1) | ((r < a) ? 0u : (r < ab ? 1u : (r < abc ? 0u : 1u)));
+            }
+            edge(k, u, v);
+        }
+    };
+    const int workers = std::max(1, std::min<int>(omp_get_max_threads() - 1, static_cast<int>(nch)));
+    const int ring = 2 * workers + 2;
+    std::vector<std::vector<uint32_t>> slot(ring, std::vector<uint32_t>(static_cast<size_t>(kChunk * per_edge)));
+    std::vector<std::atomic<int64_t>> filled(ring), done(ring);
+    for (int i = 0; i < ring; ++i) {
+        filled[i].store(-1);
+        done[i].store(static_cast<int64_t>(i) - ring);  // slot i is free for chunk i
+    }
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const int64_t ch = next.fetch_add(1);
+            if (ch >= nch) return;
+            const int sl = static_cast<int>(ch % ring);
+            while (filled[sl].load(std::memory_order_acquire) != ch) std::this_thread::yield();
+            decode(ch * kChunk, std::min(ne, (ch + 1) * kChunk), slot[sl].data());
+            done[sl].store(ch, std::memory_order_release);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < workers; ++t) pool.emplace_back(worker);
+    MtBlocks mt(seed);
+    const uint32_t *blk = nullptr;
+    int pos = MtBlocks::kN;
+    for (int64_t ch = 0; ch < nch; ++ch) {
+        const int sl = static_cast<int>(ch % ring);
+        while (done[sl].load(std::memory_order_acquire) != ch - ring) std::this_thread::yield();
+        uint32_t *dst = slot[sl].data();
+        int64_t need = (std::min(ne, (ch + 1) * kChunk) - ch * kChunk) * per_edge;
+        while (need > 0) {
+            if (pos == MtBlocks::kN) {
+                blk = mt.next_block();
+                pos = 0;
+            }
+            const int take = static_cast<int>(std::min<int64_t>(need, MtBlocks::kN - pos));
+            std::memcpy(dst, blk + pos, static_cast<size_t>(take) * sizeof(uint32_t));
+            dst += take;
+            pos += take;
+            need -= take;
+        }
+        filled[sl].store(ch, std::memory_order_release);
+    }
+    for (auto &t : pool) t.join();
+}
+
+// The weight of generated edge k: the k-th draw of uniform_int_distribution<int>(1, 255)
+// on std::mt19937(weight_seed), drawn for every generated edge in order.
+void rmat_weights(int64_t ne, uint32_t weight_seed, int32_t *w) {
+    std::mt19937 wrng(weight_seed);
+    std::uniform_int_distribution<int> W(1, 255);
+    for (int64_t k = 0; k < ne; ++k) w[k] = W(wrng);
 }
 
 }  // namespace
@@ -120,23 +270,13 @@ apspie_status apspie_gen_rmat_coo(int scale, int edge_factor, uint32_t seed, uin
     if (!src || !dst || scale < 1 || scale > 30 || edge_factor < 1) return APSPIE_ERR_INVALID_ARG;
     const int64_t ne = (int64_t(1) << scale) * edge_factor;
     if (ne > INT32_MAX) return APSPIE_ERR_UNSUPPORTED;
-    const double ab = a + b, abc = a + b + c;
-    std::mt19937 rng(seed);
-    std::uniform_real_distribution<double> U(0.0, 1.0);
-    std::mt19937 wrng(weight_seed);
-    std::uniform_int_distribution<int> W(1, 255);
-    for (int64_t k = 0; k < ne; ++k) {
-        uint32_t u = 0, v = 0;
-        for (int l = 0; l < scale; ++l) {
-            const double r = U(rng);
-            u = (u << 1) | ((r >= ab) ? 1u : 0u);
-            v = (v << 1) | ((r < a) ? 0u : (r < ab ? 1u : (r < abc ? 0u : 1u)));
-        }
-        const int wk = W(wrng);
+    std::thread wthread;
+    if (weight) wthread = std::thread(rmat_weights, ne, weight_seed, weight);
+    rmat_edges(scale, ne, seed, a, b, c, [&](int64_t k, uint32_t u, uint32_t v) {
         src[k] = static_cast<int32_t>(u);
         dst[k] = static_cast<int32_t>(v);
-        if (weight) weight[k] = wk;
-    }
+    });
+    if (wthread.joinable()) wthread.join();
     return APSPIE_OK;
 }
 
@@ -148,42 +288,47 @@ apspie_status apspie_gen_rmat(int scale, int edge_factor, uint32_t seed, uint32_
     const int64_t m = int64_t(1) << scale;
     const int64_t ne = m * edge_factor;
     if (2 * ne > INT32_MAX) return APSPIE_ERR_UNSUPPORTED;
-    const double ab = a + b, abc = a + b + c;
-    std::mt19937 rng(seed);
-    std::uniform_real_distribution<double> U(0.0, 1.0);
-    std::mt19937 wrng(weight_seed);
-    std::uniform_int_distribution<int> W(1, 255);
-    std::vector<uint64_t> key;
-    std::vector<int32_t> wt;
-    key.reserve(static_cast<size_t>(ne));
-    wt.reserve(static_cast<size_t>(ne));
-    for (int64_t k = 0; k < ne; ++k) {
-        uint64_t u = 0, v = 0;
-        for (int l = 0; l < scale; ++l) {
-            const double r = U(rng);
-            const unsigned ub = (r >= ab) ? 1u : 0u;
-            const unsigned vb = (r < a) ? 0u : (r < ab ? 1u : (r < abc ? 0u : 1u));
-            u = (u << 1) | ub;
-            v = (v << 1) | vb;
-        }
-        const int wk = W(wrng);
-        if (u == v) continue;
+    // key[k] = the canonical pair (lo << scale | hi) of generated edge k, or all ones for a
+    // self-loop (it sorts after every pair and is dropped); wt[k] = its weight draw
+    std::vector<uint64_t> key(static_cast<size_t>(ne));
+    std::vector<int32_t> wt(static_cast<size_t>(ne));
+    std::thread wthread(rmat_weights, ne, weight_seed, wt.data());
+    rmat_edges(scale, ne, seed, a, b, c, [&](int64_t k, uint32_t u, uint32_t v) {
         const uint64_t lo = std::min(u, v), hi = std::max(u, v);
-        key.push_back((lo << scale) | hi);
-        wt.push_back(wk);
-    }
+        key[k] = u == v ? ~0ull : ((lo << scale) | hi);
+    });
+    wthread.join();
     // stable sort by pair keeps generation order inside equal pairs: first copy wins
     radix_sort_pairs(key, wt, 2 * scale);
-    std::vector<uint64_t> uniq;
-    std::vector<int32_t> uw;
-    uniq.reserve(key.size());
-    uw.reserve(key.size());
+    // keep the first of every run of equal pairs (the self-loop marks sort last and go)
+    int64_t nv = ne;
+    while (nv > 0 && key[nv - 1] == ~0ull) --nv;
+    const int T = std::max(1, omp_get_max_threads());
+    std::vector<int64_t> kept(static_cast<size_t>(T) + 1, 0);
+    auto first_of_run = [&](int64_t i) { return i == 0 || key[i] != key[i - 1]; };
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num();
+        const int64_t i0 = nv * t / T, i1 = nv * (t + 1) / T;
+        int64_t n = 0;
+        for (int64_t i = i0; i < i1; ++i) n += first_of_run(i);
+        kept[t + 1] = n;
+    }
+    for (int t = 0; t < T; ++t) kept[t + 1] += kept[t];
+    std::vector<uint64_t> uniq(static_cast<size_t>(kept[T]));
+    std::vector<int32_t> uw(static_cast<size_t>(kept[T]));
     const uint64_t mask = static_cast<uint64_t>(m - 1);
-    for (size_t i = 0; i < key.size(); ++i)
-        if (i == 0 || key[i] != key[i - 1]) {
-            uniq.push_back(((key[i] >> scale) << 32) | (key[i] & mask));
-            uw.push_back(wt[i]);
-        }
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num();
+        const int64_t i0 = nv * t / T, i1 = nv * (t + 1) / T;
+        int64_t o = kept[t];
+        for (int64_t i = i0; i < i1; ++i)
+            if (first_of_run(i)) {
+                uniq[o] = ((key[i] >> scale) << 32) | (key[i] & mask);
+                uw[o++] = wt[i];
+            }
+    }
     build_symmetric(static_cast<int>(m), uniq, with_weights ? &uw : nullptr, out);
     return APSPIE_OK;
 }

@@ -186,3 +186,25 @@ def test_parallel_mtx_loader_short_file_and_errors(tmp_path):
     np.testing.assert_array_equal(a.col_ind, b.col_ind)
     with pytest.raises(ap.ApspieError):
         ap.load_mtx(str(tmp_path / "missing.mtx"), False, threads=2)
+
+
+def test_rmat_generation_is_independent_of_thread_count():
+    """The generator splits the mt19937 stream into chunks decoded by worker threads and
+    builds the CSR with per-thread offsets: one thread and many give the same bytes."""
+    import subprocess
+    import sys
+
+    code = ("import hashlib, numpy as np, apspie_b200 as ap\n"
+            "g = ap.gen_rmat(16, 16, 5, 9)\n"
+            "s, d, w = ap.gen_rmat_coo(15, 16, 5, 9)\n"
+            "h = hashlib.sha256()\n"
+            "for a in (g.row_ptr, g.col_ind, g.val, s, d, w): h.update(np.ascontiguousarray(a).tobytes())\n"
+            "print(h.hexdigest())\n")
+    digests = set()
+    for threads in ("1", "3", "8"):
+        env = dict(os.environ, OMP_NUM_THREADS=threads)
+        out = subprocess.run([sys.executable, "-c", code], env=env, cwd=ROOT, capture_output=True, text=True,
+                             timeout=300)
+        assert out.returncode == 0, out.stderr
+        digests.add(out.stdout.strip())
+    assert len(digests) == 1
