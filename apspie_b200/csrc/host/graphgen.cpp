@@ -398,29 +398,52 @@ apspie_status apspie_lcc_sample(const apspie_host_csr *g, int32_t count, uint32_
                                 int32_t *out) {
     if (!g || count < 0 || (count > 0 && !out) || g->m <= 0) return APSPIE_ERR_INVALID_ARG;
     const int32_t m = g->m;
+    // connected components by lock-free union-find over all edges in parallel: a root is
+    // only ever hooked under a smaller root, so each tree's root is its component's
+    // smallest vertex, whatever the order of the unions
     std::vector<int32_t> parent(m);
     std::iota(parent.begin(), parent.end(), 0);
-    auto find = [&](int32_t x) {
-        while (parent[x] != x) {
-            parent[x] = parent[parent[x]];
-            x = parent[x];
+    int32_t *par = parent.data();
+    auto find = [par](int32_t x) {
+        for (;;) {
+            const int32_t p = __atomic_load_n(par + x, __ATOMIC_RELAXED);
+            if (p == x) return x;
+            const int32_t gp = __atomic_load_n(par + p, __ATOMIC_RELAXED);
+            if (gp != p) {
+                int32_t expect = p;  // path halving; losing the race is harmless
+                __atomic_compare_exchange_n(par + x, &expect, gp, false, __ATOMIC_RELAXED, __ATOMIC_RELAXED);
+            }
+            x = gp;
         }
-        return x;
     };
+#pragma omp parallel for schedule(dynamic, 1024)
     for (int32_t u = 0; u < m; ++u)
         for (int32_t e = g->row_ptr[u]; e < g->row_ptr[u + 1]; ++e) {
-            int32_t a = find(u), b = find(g->col_ind[e]);
-            if (a != b) parent[std::max(a, b)] = std::min(a, b);
+            int32_t a = u, b = g->col_ind[e];
+            for (;;) {
+                a = find(a);
+                b = find(b);
+                if (a == b) break;
+                if (a > b) std::swap(a, b);
+                int32_t expect = b;  // hook the larger root under the smaller
+                if (__atomic_compare_exchange_n(par + b, &expect, a, false, __ATOMIC_ACQ_REL, __ATOMIC_RELAXED))
+                    break;
+            }
         }
+    std::vector<int32_t> comp(m);
     std::vector<int32_t> size(m, 0);
-    for (int32_t v = 0; v < m; ++v) ++size[find(v)];
+#pragma omp parallel for schedule(static)
+    for (int32_t v = 0; v < m; ++v) {
+        comp[v] = find(v);
+        __atomic_fetch_add(&size[comp[v]], 1, __ATOMIC_RELAXED);
+    }
     int32_t root = 0;
     for (int32_t v = 0; v < m; ++v)
         if (size[v] > size[root]) root = v;  // roots are component minima: ties -> smallest id
     std::vector<int32_t> lcc;
     lcc.reserve(size[root]);
     for (int32_t v = 0; v < m; ++v)
-        if (find(v) == root) lcc.push_back(v);
+        if (comp[v] == root) lcc.push_back(v);
     if (count > static_cast<int32_t>(lcc.size())) return APSPIE_ERR_INVALID_ARG;
     std::mt19937 rng(seed);
     const int64_t sz = static_cast<int64_t>(lcc.size());
