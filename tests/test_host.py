@@ -188,9 +188,10 @@ def test_parallel_mtx_loader_short_file_and_errors(tmp_path):
         ap.load_mtx(str(tmp_path / "missing.mtx"), False, threads=2)
 
 
-def test_rmat_generation_is_independent_of_thread_count():
+def test_rmat_generation_and_lcc_sample_are_independent_of_thread_count():
     """The generator splits the mt19937 stream into chunks decoded by worker threads and
-    builds the CSR with per-thread offsets: one thread and many give the same bytes."""
+    builds the CSR with per-thread offsets, and the component sample runs a parallel
+    union-find: one thread and many give the same bytes."""
     import subprocess
     import sys
 
@@ -198,7 +199,8 @@ def test_rmat_generation_is_independent_of_thread_count():
             "g = ap.gen_rmat(16, 16, 5, 9)\n"
             "s, d, w = ap.gen_rmat_coo(15, 16, 5, 9)\n"
             "h = hashlib.sha256()\n"
-            "for a in (g.row_ptr, g.col_ind, g.val, s, d, w): h.update(np.ascontiguousarray(a).tobytes())\n"
+            "smp = ap.lcc_sample(g, 64, 6)\n"
+            "for a in (g.row_ptr, g.col_ind, g.val, s, d, w, smp): h.update(np.ascontiguousarray(a).tobytes())\n"
             "print(h.hexdigest())\n")
     digests = set()
     for threads in ("1", "3", "8"):
