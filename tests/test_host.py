@@ -210,3 +210,10 @@ def test_rmat_generation_and_lcc_sample_are_independent_of_thread_count():
         assert out.returncode == 0, out.stderr
         digests.add(out.stdout.strip())
     assert len(digests) == 1
+
+
+def test_integration_guide_covers_every_declared_function():
+    """Every C-ABI function a header declares is named in the integration guide."""
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = sorted(n for n in declared_functions() if n not in guide)
+    assert not missing, missing
