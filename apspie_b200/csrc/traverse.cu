@@ -1003,20 +1003,63 @@ constexpr size_t kNaBytes =
 // kernel initialises every queue and bitmap it reads.
 static __device__ __align__(256) unsigned char g_bfs_noalloc_scratch[kNaBytes];
 
-constexpr int kNaMaxDevices = 64;
-void *g_na_ptr[kNaMaxDevices] = {};
+// A __device__ array has one address per CUDA context: the primary context of each device,
+// any context a caller made with cuCtxCreate, and a primary context re-created after
+// cudaDeviceReset each hold their own copy. The address is therefore looked up once per
+// context and cached under the context's process-unique id (cuCtxGetId), never under a
+// device number or a context handle, which a re-created context may reuse.
+struct NaEntry {
+    unsigned long long ctx_id;
+    void *addr;
+};
+std::vector<NaEntry> g_na_cache;
 std::mutex g_na_mu;
 
-// Device address of g_bfs_noalloc_scratch on the current device, looked up once per device.
-cudaError_t noalloc_scratch(int dev, void **out) {
+using CtxGetCurrentFn = int (*)(void **);              // cuCtxGetCurrent(CUcontext *)
+using CtxGetIdFn = int (*)(void *, unsigned long long *);  // cuCtxGetId(CUcontext, id *)
+
+// The id of the context current on this thread, or 0 when there is none or the driver
+// cannot say (then the address is looked up on every call, which is always right).
+unsigned long long current_ctx_id() {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault) == cudaSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault) == cudaSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+        (void)cudaGetLastError();
+    });
+    void *c = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&c) != 0 || !c || get_id(c, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of g_bfs_noalloc_scratch in the current context, looked up (with
+// cudaGetSymbolAddress, which also loads the library's device code into the context under
+// lazy module loading) on the first call in each context.
+cudaError_t noalloc_scratch(void **out) {
     std::lock_guard<std::mutex> lock(g_na_mu);
-    if (!g_na_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_na_ptr[dev] = p;
+    unsigned long long id = current_ctx_id();
+    if (id != 0)
+        for (const NaEntry &e : g_na_cache)
+            if (e.ctx_id == id) {
+                *out = e.addr;
+                return cudaSuccess;
+            }
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_bfs_noalloc_scratch);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return e;
     }
-    *out = g_na_ptr[dev];
+    if (id == 0) id = current_ctx_id();  // the lookup may have made the primary context current
+    if (id != 0) g_na_cache.push_back({id, p});
+    *out = p;
     return cudaSuccess;
 }
 
@@ -1284,9 +1327,9 @@ apspie_status apspie_bfs_noalloc(const apspie_csr *A, int32_t source, int32_t de
     if (source < 0 || source >= A->m) return APSPIE_ERR_INVALID_ARG;
     cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) return APSPIE_ERR_CUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess) return APSPIE_ERR_CUDA;
     void *base = nullptr;
-    if (noalloc_scratch(dev, &base) != cudaSuccess) return APSPIE_ERR_CUDA;
+    if (noalloc_scratch(&base) != cudaSuccess) return APSPIE_ERR_CUDA;
     char *p = static_cast<char *>(base);
     TravCtl *ctl = reinterpret_cast<TravCtl *>(p);
     int *sticky = reinterpret_cast<int *>(p + align256(sizeof(TravCtl)));

@@ -205,7 +205,11 @@ def main_reference(args, ws, rank):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/apspie_ref (the reference CPU "
                           "code compiled from its sources) was not built"}))
         return 0
-    g, src = build_graph(20, 2)
+    # the input comes from the oracle's serial restatement of the generator (the same CSR
+    # as the product's generator, pinned by tests/test_host.py), so this arm loads nothing
+    # of the product library
+    g = oracle.gen_rmat(20, 16, 2, 3)
+    src = g.max_degree_vertex()
     comp_edges = int(g.degrees()[oracle.sssp(g.row_ptr, g.col_ind, g.val, src) >= 0].sum())
     workers = ref_worker_count()
     with tempfile.TemporaryDirectory() as d:

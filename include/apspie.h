@@ -240,10 +240,16 @@ apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A, const int3
  * with no context. Its scratch (frontier queues, bitmaps, control block, about 4.3 MB) is a
  * fixed device array inside the library that every GPU which loads the library holds until
  * the process exits; graphs above APSPIE_NOALLOC_MAX_VERTICES vertices are rejected with
- * APSPIE_ERR_INVALID_ARG. The first call on a device looks the array's address up
- * (cudaGetSymbolAddress), so make that first call before any stream capture. All calls
- * share the one array: calls that overlap on the GPU (other streams, other host threads)
- * race and corrupt each other; serialise them. Synchronises `cuda_stream` and returns any
+ * APSPIE_ERR_INVALID_ARG. The first call in each CUDA context (the device's primary
+ * context, a context made with cuCtxCreate, or a primary context re-created after
+ * cudaDeviceReset) looks the array's address up with cudaGetSymbolAddress, so make that
+ * first call before any stream capture. Under lazy module loading (CUDA_MODULE_LOADING=LAZY,
+ * the default since CUDA 12.2) that first call is also what loads the library's device
+ * code and the 4.3 MB array into the context: a host that reserves all free device memory
+ * up front should make one call first (or run with CUDA_MODULE_LOADING=EAGER), else the
+ * first call can fail with APSPIE_ERR_CUDA for want of memory. All calls share the one
+ * array: calls that overlap on the GPU (other streams, other host threads) race and
+ * corrupt each other; serialise them. Synchronises `cuda_stream` and returns any
  * device-side error; `stats` may be NULL. */
 #define APSPIE_NOALLOC_MAX_VERTICES 262144
 apspie_status apspie_bfs_noalloc(const apspie_csr *A, int32_t source, int32_t depth_cap,

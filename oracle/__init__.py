@@ -48,6 +48,8 @@ def lib():
             "oracle_spgemm_fill": (None, [I, I, I, P, P, P, P, P, P, P, P, P]),
             "oracle_tc": (ctypes.c_longlong, [I, P, P]),
             "oracle_mt19937": (None, [ctypes.c_uint, ctypes.c_longlong, P]),
+            "oracle_gen_rmat": (ctypes.c_longlong, [I, I, ctypes.c_uint, ctypes.c_uint, ctypes.c_double,
+                                                    ctypes.c_double, ctypes.c_double, ctypes.c_longlong, P, P, P]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(_lib, name)
@@ -170,6 +172,36 @@ def pagerank(row_ptr, col_ind, damping=0.85, tol=1e-6, max_iter=100):
         if diff < tol:
             break
     return r, it
+
+
+class Csr:
+    """A host CSR (row_ptr, col_ind, val) from the oracle's generator."""
+
+    def __init__(self, row_ptr, col_ind, val):
+        self.row_ptr, self.col_ind, self.val = row_ptr, col_ind, val
+        self.m = self.n = row_ptr.shape[0] - 1
+        self.nnz = col_ind.shape[0]
+
+    def degrees(self):
+        return np.diff(self.row_ptr)
+
+    def max_degree_vertex(self):
+        return int(np.argmax(self.degrees()))  # argmax takes the first (smallest id) maximum
+
+
+def gen_rmat(scale, edge_factor, seed, weight_seed, a=0.57, b=0.19, c=0.19, weights=True):
+    """Serial restatement of the undirected R-MAT input (oracle/gen.cpp states the spec)."""
+    m = 1 << scale
+    rp = np.empty(m + 1, dtype=np.int32)
+    args = (scale, edge_factor, seed, weight_seed, a, b, c)
+    need = lib().oracle_gen_rmat(*args, 0, _p(rp), None, None)
+    if need < 0:
+        raise ValueError("oracle_gen_rmat: bad arguments")
+    ci = np.empty(need, dtype=np.int32)
+    w = np.empty(need, dtype=np.int32) if weights else None
+    got = lib().oracle_gen_rmat(*args, need, _p(rp), _p(ci), _p(w) if weights else None)
+    assert got == need
+    return Csr(rp, ci, w)
 
 
 def mt19937(seed, count):

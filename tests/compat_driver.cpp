@@ -3,7 +3,7 @@
 //   compat_driver <outdir>
 // Builds R-MAT scale 12 (seed 1, weights seed 3) with the library's host generator, loads
 // it through matrix_new/buildMatrix from COO, runs bfs<int>, spmspvBfs, sssp<int>,
-// sssp<float>, spmspvMis<float>, spmspvCsr, spgemm(d_matrix*) and triangleCount, and writes
+// sssp<float>, spmspvMis<float>, spmspvCsr, spgemm(d_matrix*), mXm and triangleCount, and writes
 // each result as a raw binary file for the test to compare with the oracle.
 #include <cstdio>
 #include <string>
@@ -83,6 +83,37 @@ int main(int argc, char **argv) {
     dump(out + "/spgemm_ci.i32", C.d_cscRowInd, static_cast<size_t>(C.nnz) * sizeof(int));
     dump(out + "/spgemm_v.f32", C.d_cscVal, static_cast<size_t>(C.nnz) * sizeof(float));
 
+    // mXm (src/tc.cuh:315) on two different matrices over CSC arrays: A's CSC arrays are
+    // the R-MAT's CSR arrays (so A = R^T) and B's are an Erdos-Renyi matrix E's (B = E^T);
+    // the CSC of C = A*B is then the CSR of E*R, which the test checks.
+    apspie_host_csr er;
+    if (apspie_gen_er(m, 8, 9, APSPIE_VAL_F32, &er) != APSPIE_OK) return 4;
+    int *d_erp = nullptr, *d_eci = nullptr;
+    float *d_ev = nullptr;
+    cudaMalloc(&d_erp, (m + 1) * sizeof(int));
+    cudaMalloc(&d_eci, er.nnz * sizeof(int));
+    cudaMalloc(&d_ev, er.nnz * sizeof(float));
+    cudaMemcpy(d_erp, er.row_ptr, (m + 1) * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_eci, er.col_ind, er.nnz * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_ev, er.val, er.nnz * sizeof(float), cudaMemcpyHostToDevice);
+    const size_t cap = static_cast<size_t>(er.nnz) * 64;  // >= products of E*R
+    int *d_cp = nullptr, *d_cr = nullptr;
+    float *d_cv = nullptr;
+    cudaMalloc(&d_cp, (m + 1) * sizeof(int));
+    cudaMalloc(&d_cr, cap * sizeof(int));
+    cudaMalloc(&d_cv, cap * sizeof(float));
+    const int nnz_c = mXm<float>(edge, m, A.d_cscVal, A.d_cscColPtr, A.d_cscRowInd, d_ev, er.row_ptr, d_erp, d_eci,
+                                 d_cv, d_cp, d_cr, *context);
+    dump(out + "/mxm_rp.i32", d_cp, (m + 1) * sizeof(int));
+    dump(out + "/mxm_ci.i32", d_cr, static_cast<size_t>(nnz_c) * sizeof(int));
+    dump(out + "/mxm_v.f32", d_cv, static_cast<size_t>(nnz_c) * sizeof(float));
+    cudaFree(d_erp);
+    cudaFree(d_eci);
+    cudaFree(d_ev);
+    cudaFree(d_cp);
+    cudaFree(d_cr);
+    cudaFree(d_cv);
+
     long long tri = triangleCount(edge, m, A.d_cscColPtr, A.d_cscRowInd, *context);
     FILE *tf = std::fopen((out + "/tc.txt").c_str(), "w");
     std::fprintf(tf, "%lld\n", tri);
@@ -92,5 +123,6 @@ int main(int argc, char **argv) {
     matrix_delete(&A);
     matrix_delete(&C);
     apspie_host_csr_free(&g);
+    apspie_host_csr_free(&er);
     return e == cudaSuccess ? 0 : 1;
 }

@@ -1,7 +1,7 @@
 """Generates tests/golden/golden.npz from the REFERENCE's own CPU code.
 
 Run here, where the reference tree and oracle/_ref/apspie_ref (built by `make -C oracle`)
-exist:  python tests/golden/make_golden.py [REF_DIR]
+exist:  python tests/golden/make_golden.py REF_DIR   (or REF_DIR in the environment)
 
 Contents, per small Matrix Market fixture of the reference (dataset/small/*.mtx) and
 both load modes (directed / undirected = makeSymmetric):
@@ -59,9 +59,12 @@ def csr_digest(rp, ci, val=None):
     return h.hexdigest()
 
 
-def main(ref_dir="/root/reference"):
+def main(ref_dir=None):
+    ref_dir = ref_dir or os.environ.get("REF_DIR")
+    if not ref_dir or not os.path.isdir(os.path.join(ref_dir, "dataset")):
+        raise SystemExit("give the reference source tree: make_golden.py REF_DIR")
     if not oracle.ref_available():
-        raise SystemExit("oracle/_ref/apspie_ref missing: run `make -C oracle` first")
+        raise SystemExit("oracle/_ref/apspie_ref missing: run `make -C oracle REF_DIR=...` first")
     out = {}
     manifest = {"fixtures": []}
     for path in sorted(glob.glob(os.path.join(ref_dir, "dataset", "small", "*.mtx"))):

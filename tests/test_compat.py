@@ -55,5 +55,12 @@ def test_compat_driver_matches_oracle(tmp_path):
     np.testing.assert_array_equal(rd("spgemm_rp.i32", np.int32), orp)
     np.testing.assert_array_equal(rd("spgemm_ci.i32", np.int32), oci)
     np.testing.assert_allclose(rd("spgemm_v.f32", np.float32), ocv, rtol=1e-5)
+    er = ap.gen_er(g.m, 8, 9, ap.VAL_F32)
+    orp, oci, ocv = oracle.spgemm(g.m, g.m, er.row_ptr, er.col_ind, er.val, g.row_ptr, g.col_ind, vals)
+    np.testing.assert_array_equal(rd("mxm_rp.i32", np.int32), orp)  # mXm: CSC of R^T * E^T = CSR of E * R
+    np.testing.assert_array_equal(rd("mxm_ci.i32", np.int32), oci)
+    # rows of E*R reach hundreds of signed products: the f32 bar is |got - ref| <= 1e-5 * sum|a*b|
+    _, _, mag = oracle.spgemm(g.m, g.m, er.row_ptr, er.col_ind, np.abs(er.val), g.row_ptr, g.col_ind, vals)
+    assert np.all(np.abs(rd("mxm_v.f32", np.float32) - ocv) <= 1e-5 * mag)
     L = ap.strict_lower(g)
     assert int(open(os.path.join(outdir, "tc.txt")).read()) == oracle.tc(L.row_ptr, L.col_ind)

@@ -87,13 +87,16 @@ def test_server_budget_enforced(graphs):
 
 def test_server_tight_budget_shrinks_batches_but_answers_stay_exact(ctx, graphs):
     g = graphs[2]
-    probe = ap.Server(0, budget_bytes=4 << 30, slots=1)
+    # A one-query server reserves the graph plus the arena of a one-word (<= 32 query)
+    # batch. 64 KB more than that lets the tight server's arena grow to a one-word batch
+    # but not to the two-word arena (12 bytes per vertex more) that 64 sources would need.
+    probe = ap.Server(0, budget_bytes=4 << 30, slots=1, max_batch=1)
     probe.add_graph(g)
     probe.start()
     resident = probe.stats()["resident_bytes"]
     probe.close()
-    # room for the graph, the slot's scratch and about ten BFS output rows at a time
-    budget = resident + 10 * g.m * 4 + 4096
+    budget = resident + (64 << 10)
+    assert 12 * g.m > 2 * (64 << 10)
     srv = ap.Server(0, budget_bytes=budget, slots=1, max_batch=512)
     gid = srv.add_graph(g)
     srv.start()
