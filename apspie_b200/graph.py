@@ -346,6 +346,21 @@ class Context:
         self._check(L.lib().apspie_spmspv_bool(self.handle, ctypes.byref(g.view(False)),
                                                x.data_ptr(), y.data_ptr()), "spmspv_bool")
 
+    def spmspv(self, g: DeviceGraph, x_ind, x_val):
+        """y = x^T A for a sparse x (x_ind int32, x_val of A's value type, CUDA tensors);
+        returns (y_ind, y_val) CUDA tensors of y's entries, indices ascending."""
+        import torch
+
+        nx = int(x_ind.shape[0])
+        cap = max(1, min(g.n, g.nnz))
+        y_ind = torch.empty(cap, dtype=torch.int32, device=x_ind.device)
+        y_val = torch.empty(cap, dtype=x_val.dtype, device=x_ind.device)
+        ny = ctypes.c_int32(0)
+        self._check(L.lib().apspie_spmspv(self.handle, ctypes.byref(g.view(True)), x_ind.data_ptr(),
+                                          x_val.data_ptr(), nx, y_ind.data_ptr(), y_val.data_ptr(),
+                                          ctypes.byref(ny)), "spmspv")
+        return y_ind[: ny.value], y_val[: ny.value]
+
     # ---- batched traversal
     def bfs_batch_into(self, g: DeviceGraph, sources, out, depth_cap: int = 0, stats: bool = False):
         """sources: int32 CUDA tensor [nq]; out: int32 CUDA tensor [nq, m] (query-major)."""

@@ -274,6 +274,19 @@ apspie_status apspie_mis_int32(apspie_ctx *ctx, const apspie_csr *A, const uint3
 apspie_status apspie_spmspv_bool(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_x,
                                  int32_t *d_y);
 
+/* Valued sparse-in / sparse-out SpMSpV y = x^T A: x has x_nnz entries (row index
+ * d_x_ind[j] of A, value d_x_val[j], in A's value type, F32 or I32; repeated indices add);
+ * y gets one entry per column that some product lands in, d_y_ind ascending and d_y_val
+ * the sum of that column's products (a column whose products cancel keeps a 0 entry), and
+ * *y_nnz their number. d_y_ind / d_y_val must hold min(n, sum of x's row lengths)
+ * entries. Each sum is taken in x's entry order, then A's row order, with correctly
+ * rounded f32 multiplies and adds (no fused multiply-add; int32 wraps), so it is
+ * bit-identical to that sequential loop. Synchronises the context's stream. Replaces
+ * mXv<T> (src/mXv.cuh:249-389: IntervalGather of the vector's CSC columns, elementMult,
+ * SortPairs, ReduceByKey). An index outside [0, m) is APSPIE_ERR_INVALID_ARG. */
+apspie_status apspie_spmspv(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_x_ind, const void *d_x_val,
+                            int32_t x_nnz, int32_t *d_y_ind, void *d_y_val, int32_t *y_nnz);
+
 /* ---- SpGEMM and triangle counting ---------------------------------------------- */
 
 /* C = A * B, row-binned hash Gustavson. A and B share val_type (F32 or I32). C's rows are

@@ -236,6 +236,35 @@ void spmspvCsr(const T *d_inputVector, const int edge, const int m, const int *d
                           context, "spmspvCsr");
 }
 
+// src/scratch.hpp:5-31 / src/util.cuh:646-672: the reference's per-call scratch block. The
+// context owns all scratch here, so the block carries nothing; allocScratch / freeScratch
+// keep programs that create and pass one compiling.
+struct d_scratch {};
+inline void allocScratch(d_scratch **d, const int edge, const int m) {
+    (void)edge;
+    (void)m;
+    *d = new d_scratch();
+}
+inline void freeScratch(d_scratch *d) { delete d; }
+
+// src/mXv.cuh:249: sparse vector (d_randVecInd, d_randVecVal, nnz entries) times the CSC
+// matrix (column j = d_cscRowInd[d_cscColPtr[j] ..]); the result's indices go to d_resultInd
+// ascending with summed values in d_resultVal, and nnz becomes their number. Over the same
+// arrays read as CSR this is y = x^T A.
+template <typename T>
+void mXv(const int *d_randVecInd, const T *d_randVecVal, const int edge, const int m, int &nnz, const T *d_cscVal,
+         const int *d_cscColPtr, const int *d_cscRowInd, int *d_resultInd, T *d_resultVal, d_scratch *d,
+         mgpu::CudaContext &context) {
+    (void)d;
+    apspie_csr a = apspie_compat::view(m, m, edge, d_cscColPtr, d_cscRowInd, d_cscVal,
+                                       apspie_compat::ValType<T>::value, false);
+    int32_t ny = 0;
+    if (apspie_compat::report(apspie_spmspv(context.get(), &a, d_randVecInd, d_randVecVal, nnz, d_resultInd,
+                                            d_resultVal, &ny),
+                              context, "mXv"))
+        nnz = ny;
+}
+
 // ---------------------------------------------------------------------------------
 // SpGEMM and triangle counting
 // ---------------------------------------------------------------------------------

@@ -48,6 +48,7 @@ def lib():
             "oracle_spgemm_fill": (None, [I, I, I, P, P, P, P, P, P, P, P, P]),
             "oracle_tc": (ctypes.c_longlong, [I, P, P]),
             "oracle_mt19937": (None, [ctypes.c_uint, ctypes.c_longlong, P]),
+            "oracle_spmspv": (I, [I, I, I, P, P, P, I, P, P, P, P]),
             "oracle_gen_rmat": (ctypes.c_longlong, [I, I, ctypes.c_uint, ctypes.c_uint, ctypes.c_double,
                                                     ctypes.c_double, ctypes.c_double, ctypes.c_longlong, P, P, P]),
         }
@@ -133,6 +134,21 @@ def spgemm(m, n, arp, aci, aval, brp, bci, bval):
                              _p(brp), _p(bci), None if bv is None else _p(bv), _p(crp),
                              _p(cci), None if cval is None else _p(cval))
     return crp, cci[:nnz], None if cval is None else cval[:nnz]
+
+
+def spmspv(row_ptr, col_ind, val, n, x_ind, x_val):
+    """y = x^T A (sparse in, sparse out); returns (y_ind, y_val)."""
+    rp, ci = _i32(row_ptr), _i32(col_ind)
+    vt = 1 if np.asarray(val).dtype == np.float32 else 2
+    dt = np.float32 if vt == 1 else np.int32
+    av = np.ascontiguousarray(val, dtype=dt)
+    xi = _i32(x_ind)
+    xv = np.ascontiguousarray(x_val, dtype=dt)
+    y_ind = np.empty(max(1, n), dtype=np.int32)
+    y_val = np.empty(max(1, n), dtype=dt)
+    k = lib().oracle_spmspv(rp.shape[0] - 1, n, vt, _p(rp), _p(ci), _p(av), xi.shape[0], _p(xi), _p(xv),
+                            _p(y_ind), _p(y_val))
+    return y_ind[:k].copy(), y_val[:k].copy()
 
 
 def tc(row_ptr_l, col_ind_l):

@@ -288,3 +288,43 @@ void oracle_mt19937(unsigned seed, long long count, unsigned *out) {
         out[c] = y;
     }
 }
+
+/* Sparse vector times matrix, y = x^T A (the reference's mXv<T>, src/mXv.cuh:249-389:
+ * gather the vector's rows, multiply, sort by column, sum runs of equal columns). Each
+ * column's sum runs in x's entry order, then row order, starting from 0. vt 1: f32 (no
+ * contraction: this file is built with -ffp-contract=off), 2: int32 (wrapping). Writes the
+ * touched columns ascending into y_ind / y_val and returns their number. */
+int oracle_spmspv(int m, int n, int vt, const int *rp, const int *ci, const void *aval, int nx, const int *x_ind,
+                  const void *x_val, int *y_ind, void *y_val) {
+    unsigned char *hit = (unsigned char *)calloc((size_t)(n > 0 ? n : 1), 1);
+    float *accf = (float *)calloc((size_t)(n > 0 ? n : 1), sizeof(float));
+    unsigned *acci = (unsigned *)calloc((size_t)(n > 0 ? n : 1), sizeof(unsigned));
+    (void)m;
+    for (int j = 0; j < nx; ++j) {
+        const int r = x_ind[j];
+        for (int e = rp[r]; e < rp[r + 1]; ++e) {
+            const int c = ci[e];
+            hit[c] = 1;
+            if (vt == 1) {
+                const float p = ((const float *)x_val)[j] * ((const float *)aval)[e];
+                accf[c] = accf[c] + p;
+            } else {
+                acci[c] += ((const unsigned *)x_val)[j] * ((const unsigned *)aval)[e];
+            }
+        }
+    }
+    int k = 0;
+    for (int c = 0; c < n; ++c)
+        if (hit[c]) {
+            y_ind[k] = c;
+            if (vt == 1)
+                ((float *)y_val)[k] = accf[c];
+            else
+                ((unsigned *)y_val)[k] = acci[c];
+            ++k;
+        }
+    free(hit);
+    free(accf);
+    free(acci);
+    return k;
+}

@@ -19,6 +19,8 @@ void oracle_spgemm_fill(int m, int n, int vt, const int *arp, const int *aci, co
                         void *cval);
 long long oracle_tc(int m, const int *rp, const int *ci);
 void oracle_mt19937(unsigned seed, long long count, unsigned *out);
+int oracle_spmspv(int m, int n, int vt, const int *rp, const int *ci, const void *aval, int nx, const int *x_ind,
+                  const void *x_val, int *y_ind, void *y_val);
 
 #ifdef __cplusplus
 }

@@ -3,7 +3,7 @@
 //   compat_driver <outdir>
 // Builds R-MAT scale 12 (seed 1, weights seed 3) with the library's host generator, loads
 // it through matrix_new/buildMatrix from COO, runs bfs<int>, spmspvBfs, sssp<int>,
-// sssp<float>, spmspvMis<float>, spmspvCsr, spgemm(d_matrix*), mXm and triangleCount, and writes
+// sssp<float>, spmspvMis<float>, spmspvCsr, spgemm(d_matrix*), mXm, mXv and triangleCount, and writes
 // each result as a raw binary file for the test to compare with the oracle.
 #include <cstdio>
 #include <string>
@@ -113,6 +113,37 @@ int main(int argc, char **argv) {
     cudaFree(d_cp);
     cudaFree(d_cr);
     cudaFree(d_cv);
+
+    // mXv (src/mXv.cuh:249): a sparse vector of 64 entries (indices 7 * k mod m, values
+    // 0.5 + k / 64, index 0 twice) times A, through the reference's scratch block
+    {
+        std::vector<int> xi(64);
+        std::vector<float> xv(64);
+        for (int k = 0; k < 64; ++k) {
+            xi[k] = (7 * k) % m;
+            xv[k] = 0.5f + k / 64.0f;
+        }
+        xi[63] = 0;
+        int *d_xi = nullptr, *d_yi = nullptr;
+        float *d_xv = nullptr, *d_yv = nullptr;
+        cudaMalloc(&d_xi, 64 * sizeof(int));
+        cudaMalloc(&d_xv, 64 * sizeof(float));
+        cudaMalloc(&d_yi, m * sizeof(int));
+        cudaMalloc(&d_yv, m * sizeof(float));
+        cudaMemcpy(d_xi, xi.data(), 64 * sizeof(int), cudaMemcpyHostToDevice);
+        cudaMemcpy(d_xv, xv.data(), 64 * sizeof(float), cudaMemcpyHostToDevice);
+        d_scratch *scr = nullptr;
+        allocScratch(&scr, edge, m);
+        int nnz_y = 64;
+        mXv<float>(d_xi, d_xv, edge, m, nnz_y, A.d_cscVal, A.d_cscColPtr, A.d_cscRowInd, d_yi, d_yv, scr, *context);
+        freeScratch(scr);
+        dump(out + "/mxv_i.i32", d_yi, static_cast<size_t>(nnz_y) * sizeof(int));
+        dump(out + "/mxv_v.f32", d_yv, static_cast<size_t>(nnz_y) * sizeof(float));
+        cudaFree(d_xi);
+        cudaFree(d_xv);
+        cudaFree(d_yi);
+        cudaFree(d_yv);
+    }
 
     long long tri = triangleCount(edge, m, A.d_cscColPtr, A.d_cscRowInd, *context);
     FILE *tf = std::fopen((out + "/tc.txt").c_str(), "w");

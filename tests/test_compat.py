@@ -62,5 +62,11 @@ def test_compat_driver_matches_oracle(tmp_path):
     # rows of E*R reach hundreds of signed products: the f32 bar is |got - ref| <= 1e-5 * sum|a*b|
     _, _, mag = oracle.spgemm(g.m, g.m, er.row_ptr, er.col_ind, np.abs(er.val), g.row_ptr, g.col_ind, vals)
     assert np.all(np.abs(rd("mxm_v.f32", np.float32) - ocv) <= 1e-5 * mag)
+    xi = (7 * np.arange(64)) % g.m
+    xi[63] = 0
+    xv = (0.5 + np.arange(64) / 64.0).astype(np.float32)
+    oi, ov = oracle.spmspv(g.row_ptr, g.col_ind, vals, g.m, xi, xv)
+    np.testing.assert_array_equal(rd("mxv_i.i32", np.int32), oi)  # mXv: bit-exact, same summation order
+    np.testing.assert_array_equal(rd("mxv_v.f32", np.float32), ov)
     L = ap.strict_lower(g)
     assert int(open(os.path.join(outdir, "tc.txt")).read()) == oracle.tc(L.row_ptr, L.col_ind)

@@ -1,84 +1,109 @@
 """A CPU model of the MIS kernel's round protocol under random interleavings: it reaches
 the oracle's set (the greedy MIS in descending (priority, id) order) on every schedule, and
-a model with a planted mistake does not.
+models with a planted mistake do not.
 
-Modelled at the level that matters for correctness (mis_kernel): each round's edge pass
-reads the state of every undecided vertex's neighbours while other warps of the same pass
-already mark vertices "out" (a vertex with a neighbour in the set); a row may be split
-over several tiles, each flushing its own flags (out, or blocked in this round). The
-vertex pass then lets every undecided vertex that is neither out nor blocked join. No GPU
-is involved."""
+Modelled at the level that matters for correctness (mis_kernel): each undecided vertex keeps
+a scan position (the neighbour blocking it). Phase A re-checks the blocker; a vertex whose
+blocker went out (or that has none yet) scans the rest of its row. In phase B the vertices
+that joined last round write "out" into their neighbours while, interleaved at random with
+those writes, the scans read their neighbours' states in tiles of 1-3 edges, each tile
+flushing the least stop it saw into the vertex's `first` after its own reads. Phase C lets a
+scanned vertex with no stop join and gives one with a stop its new blocker. No GPU is
+involved."""
 import numpy as np
 import pytest
 
 import oracle
 from test_batch_sssp_model import _random_graph
 
-UNDECIDED, IN, OUT = 0, 1, 2
+UNDECIDED, IN, OUT, SCAN = 0, 1, 2, 3
+INF = 1 << 60
 
 
 def _outranks(pu, u, pv, v):
     return pu > pv or (pu == pv and u > v)
 
 
-def _run_model(rp, ci, prio, rng, join_when_blocked=False):
+def _run_model(rp, ci, prio, rng, mistake=None):
     n = len(rp) - 1
     state = np.full(n, UNDECIDED)
-    blocked = np.zeros(n, dtype=np.int64)
-    queue = list(range(n))
-    for rnd in range(1, n + 3):
+    pos = np.array([int(rp[v]) - 1 for v in range(n)], dtype=np.int64)
+    first = np.full(n, INF, dtype=np.int64)
+    queue = [(v, False) for v in range(n)]  # (vertex, joined last round)
+    for _ in range(n + 3):
         if not queue:
             return state
-        # edge pass: each row cut into tiles of 1-3 edges; a tile's reads happen at random
-        # times, its flag flush happens after its own reads
+        # phase A
+        segs = []
+        for v, joined in queue:
+            r0, r1 = int(rp[v]), int(rp[v + 1])
+            if joined:
+                segs.append((v, True, r0, r1))
+                continue
+            p = int(pos[v])
+            scan = p < r0 or state[int(ci[p])] == OUT
+            if mistake == "skip_undecided_blocker" and p >= r0 and state[int(ci[p])] == UNDECIDED:
+                scan = True
+            if scan:
+                state[v] = SCAN
+                segs.append((v, False, p + 1, r1))
+        # phase B: push writes and scan tiles, interleaved at random
+        events = []
         tiles = []
-        for v in queue:
-            e, e1 = int(rp[v]), int(rp[v + 1])
+        for v, joined, e0, e1 in segs:
+            e = e0
             while e < e1:
                 k = int(rng.integers(1, 4))
-                tiles.append((v, list(range(e, min(e + k, e1)))))
+                edges = list(range(e, min(e + k, e1)))
                 e += k
-        events = [(t, "read") for t in range(len(tiles))] + [(t, "flush") for t in range(len(tiles))]
-        flags = [0] * len(tiles)
-        read = [False] * len(tiles)
-        waiting = set()
-        for k in rng.permutation(len(events)):
-            t, kind = events[k]
-            if kind == "read":
-                v, edges = tiles[t]
-                for e in edges:
-                    u = int(ci[e])
-                    if u == v:
-                        continue
-                    if state[u] == IN:
-                        flags[t] |= 1
-                    elif state[u] == UNDECIDED and _outranks(prio[u], u, prio[v], v):
-                        flags[t] |= 2
-                read[t] = True
-                if t in waiting:
-                    waiting.discard(t)
-                    _flush(tiles[t][0], flags[t], state, blocked, rnd)
-            elif read[t]:
-                _flush(tiles[t][0], flags[t], state, blocked, rnd)
-            else:
-                waiting.add(t)
-        # vertex pass
-        nxt = []
-        for v in queue:
-            if state[v] == UNDECIDED:
-                if blocked[v] != rnd or join_when_blocked:
-                    state[v] = IN
+                if joined:
+                    for x in edges:
+                        events.append(("push", v, x))
                 else:
-                    nxt.append(v)
+                    tiles.append([v, edges, INF])
+                    t = len(tiles) - 1
+                    events.append(("read", t, None))
+                    events.append(("flush", t, None))
+        pending = set()
+        done_read = set()
+        for k in rng.permutation(len(events)):
+            kind, a, b = events[k]
+            if kind == "push":
+                u = int(ci[b])
+                if u != a:
+                    state[u] = OUT
+            elif kind == "read":
+                v, edges, _ = tiles[a]
+                for x in edges:
+                    u = int(ci[x])
+                    if u != v and state[u] != OUT and _outranks(prio[u], u, prio[v], v):
+                        tiles[a][2] = min(tiles[a][2], x)
+                done_read.add(a)
+                if a in pending:
+                    pending.discard(a)
+                    first[v] = min(first[v], tiles[a][2])
+            elif a in done_read:
+                first[tiles[a][0]] = min(first[tiles[a][0]], tiles[a][2])
+            else:
+                pending.add(a)
+        # phase C
+        nxt = []
+        for v, joined in queue:
+            if joined:
+                continue
+            if state[v] == UNDECIDED:
+                nxt.append((v, False))
+            elif state[v] == SCAN:
+                if first[v] == INF or mistake == "join_despite_stop":
+                    state[v] = IN
+                    nxt.append((v, True))
+                else:
+                    pos[v] = first[v]
+                    first[v] = INF
+                    state[v] = UNDECIDED
+                    nxt.append((v, False))
         queue = nxt
     raise AssertionError("no fixed point")
-
-
-def _flush(v, f, state, blocked, rnd):
-    if f & 1:
-        state[v] = OUT
-    elif f & 2:
-        blocked[v] = rnd
 
 
 @pytest.mark.parametrize("seed", range(16))
@@ -92,15 +117,16 @@ def test_round_protocol_reaches_the_greedy_mis(seed):
     np.testing.assert_array_equal(got, oracle.mis_greedy(rp, ci, prio))
 
 
-def test_joining_while_blocked_breaks_independence():
-    """Planted mistake: a blocked vertex joins anyway; some schedule then puts two
-    neighbours in the set."""
+@pytest.mark.parametrize("mistake", ["skip_undecided_blocker", "join_despite_stop"])
+def test_planted_mistakes_break_the_set(mistake):
+    """Planted mistakes: a vertex scans past a blocker that is still undecided, or joins
+    although its scan found a stop; some schedule then puts two neighbours in the set."""
     bad = 0
     for seed in range(20):
         rng = np.random.default_rng(3000 + seed)
         rp, ci, _ = _random_graph(rng, 30, 3)
         prio = rng.integers(0, 1000, len(rp) - 1).astype(np.uint32)
-        state = _run_model(rp, ci, prio, rng, join_when_blocked=True)
+        state = _run_model(rp, ci, prio, rng, mistake=mistake)
         got = (state == IN).astype(np.uint8)
         bad += int(not np.array_equal(got, oracle.mis_greedy(rp, ci, prio)))
     assert bad > 0

@@ -234,3 +234,22 @@ def test_oracle_pagerank_and_spmv_sanity():
     assert abs(r.sum() - 1.0) < 1e-12 and r[3] > r[0]
     np.testing.assert_allclose(oracle.spmv(np.array([0, 2, 3]), np.array([0, 1, 1]), np.array([1.0, 2.0, 3.0]),
                                            np.array([1.0, 10.0])), [21.0, 30.0])
+
+
+def test_oracle_spmspv_against_dense_product():
+    """The oracle's sparse-vector product equals x^T A computed densely (int32, exact)."""
+    rng = np.random.default_rng(5)
+    n = 40
+    dense = (rng.random((n, n)) < 0.15) * rng.integers(1, 9, (n, n))
+    rp = np.concatenate([[0], np.cumsum((dense != 0).sum(1))]).astype(np.int32)
+    ci = np.nonzero(dense)[1].astype(np.int32)
+    val = dense[dense != 0].astype(np.int32)
+    x_ind = rng.integers(0, n, 12).astype(np.int32)
+    x_val = rng.integers(-3, 4, 12).astype(np.int32)
+    xd = np.zeros(n, dtype=np.int64)
+    np.add.at(xd, x_ind, x_val)
+    y = xd @ dense
+    hit = (np.abs(dense[np.unique(x_ind)]).sum(0) > 0)
+    yi, yv = oracle.spmspv(rp, ci, val, n, x_ind, x_val)
+    np.testing.assert_array_equal(yi, np.nonzero(hit)[0])
+    np.testing.assert_array_equal(yv, y[hit])
