@@ -119,6 +119,8 @@ SIGNATURES = {
     "apspie_tune_save": (c_int, [c_void_p, c_char_p]),
     "apspie_tune_load": (c_int, [c_void_p, c_char_p]),
     "apspie_ctx_set_max_grid": (c_int, [c_void_p, c_int32]),
+    "apspie_ctx_set_wait_limit": (c_int, [c_void_p, c_int64]),
+    "apspie_grid_barrier_check": (c_int, [c_void_p, c_int32, c_int32, POINTER(c_int32)]),
     "apspie_ctx_set_batch_push_frac": (c_int, [c_void_p, c_float]),
     "apspie_ctx_scratch_bytes": (c_int64, [c_void_p]),
     "apspie_ctx_timeline": (c_int, [c_void_p, c_void_p, c_void_p, c_int32, POINTER(c_int32)]),

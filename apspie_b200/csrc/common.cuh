@@ -26,6 +26,7 @@ struct TravCtl {
     unsigned bar;
     int err;             // first apspie_status error raised on the device
     int err_where;       // kernel-defined location code of that error
+    unsigned long long wait_limit_ns;  // bound of every grid-barrier wait (0: kBarrierTimeoutNs)
     int qlen[2];         // frontier queue lengths (ping-pong)
     int iterations;
     int push_iterations;
@@ -50,7 +51,8 @@ constexpr size_t kCtlHostBytes = offsetof(TravCtl, sbase);
 
 // Upper bound on a persistent grid (chunk sums are staged in shared memory).
 constexpr int kMaxGrid = 1024;
-// A grid barrier gives up after this long (ns) and raises APSPIE_ERR_TIMEOUT.
+// A grid barrier gives up after this long (ns) and raises APSPIE_ERR_TIMEOUT, unless the
+// context sets another bound (apspie_ctx_set_wait_limit).
 constexpr unsigned long long kBarrierTimeoutNs = 4000000000ull;
 
 }  // namespace apspie
@@ -104,6 +106,8 @@ struct apspie_ctx {
     int tc_orient = 1;              // TC: re-orient L by degree
     int sssp_batch_groups = 0;      // batched SSSP: <= 0 multi-query kernel, > 0 query groups
     int use_tuning = 1;             // consult tune_table
+    unsigned long long wait_limit_ns = 0;  // grid-barrier wait bound (0: kBarrierTimeoutNs)
+    unsigned long long *h_limit = nullptr;  // pinned copy of it, the source of the per-call upload
     std::vector<apspie_tune_entry> tune_table;
 };
 
@@ -130,6 +134,9 @@ int persistent_cap(const apspie_ctx *ctx, int per_sm);
 // `work` (edges the graph holds) sizes the grid: about one block per kWorkPerBlock edges,
 // at least one per SM, at most the co-resident limit (barrier cost grows with blocks).
 constexpr long long kWorkPerBlock = 4096;
+// Clears the control block on the context's stream before a launch and, when the context
+// sets its own wait bound, writes that bound into it.
+apspie_status reset_ctl(apspie_ctx *ctx);
 apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, void **args,
                                 long long work, int *grid_out = nullptr);
 // Copies the control block back, synchronises, and turns a device error into a status.
@@ -236,7 +243,8 @@ __device__ __forceinline__ VGrid hw_grid() { return VGrid{static_cast<int>(block
 // 2^31 - (G - 1); the G additions sum to 2^31, so bit 31 flips exactly when the last block
 // arrives and the low bits return to where they were (no reset). A waiter polls the pair
 // (bar, err) with one 64-bit load until bit 31 differs from what it saw before arriving,
-// or until an error is posted. Every wait is bounded by kBarrierTimeoutNs; on timeout it
+// or until an error is posted. Every wait is bounded (the control block's wait_limit_ns,
+// else kBarrierTimeoutNs); on timeout it
 // raises APSPIE_ERR_TIMEOUT. Returns false when any block has raised an error, so that all
 // blocks leave the persistent loop together instead of hanging.
 // With a VGrid group, the group's blocks synchronise on the group's own control block.
@@ -249,6 +257,7 @@ __device__ __forceinline__ bool grid_barrier(TravCtl *ctl, int *sticky, int wher
         const unsigned before = atomicAdd(&ctl->bar, inc);
         unsigned long long pair;
         unsigned long long t0 = 0;
+        const unsigned long long limit = ctl->wait_limit_ns ? ctl->wait_limit_ns : kBarrierTimeoutNs;
         for (unsigned spin = 1;; ++spin) {
             pair = ld_acquire_u64(&ctl->bar);
             if (((static_cast<unsigned>(pair) ^ before) & 0x80000000u) != 0u) break;
@@ -257,7 +266,7 @@ __device__ __forceinline__ bool grid_barrier(TravCtl *ctl, int *sticky, int wher
                 const unsigned long long t = globaltimer_ns();
                 if (t0 == 0) {
                     t0 = t;
-                } else if (t - t0 > kBarrierTimeoutNs) {
+                } else if (t - t0 > limit) {
                     raise_error(ctl, sticky, APSPIE_ERR_TIMEOUT, where);
                     pair = 1ull << 32;
                     break;

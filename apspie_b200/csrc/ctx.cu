@@ -134,6 +134,22 @@ apspie_status validate_csr(apspie_ctx *ctx, const apspie_csr *A, bool need_squar
     return APSPIE_OK;
 }
 
+apspie_status reset_ctl(apspie_ctx *ctx) {
+    cudaError_t e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(TravCtl), ctx->stream);
+    if (e == cudaSuccess && ctx->wait_limit_ns != 0)
+        e = cudaMemcpyAsync(&ctx->d_ctl->wait_limit_ns, ctx->h_limit, sizeof(unsigned long long),
+                            cudaMemcpyHostToDevice, ctx->stream);
+    return e == cudaSuccess ? APSPIE_OK : cuda_error(ctx, e, "control reset");
+}
+
+// A cooperative grid that passes `rounds` grid barriers; block `absent` (when >= 0) leaves
+// before its first arrival, so the others' first wait runs out.
+__global__ void barrier_check_kernel(TravCtl *ctl, int *sticky, int rounds, int absent) {
+    if (static_cast<int>(blockIdx.x) == absent) return;
+    for (int r = 0; r < rounds; ++r)
+        if (!grid_barrier(ctl, sticky, 900 + r)) return;
+}
+
 int persistent_cap(const apspie_ctx *ctx, int per_sm) {
     // a context that shares the device with grid_share - 1 others takes 1/grid_share of the
     // co-resident capacity, so that all of them fit at once. Whole blocks per SM: then each
@@ -215,6 +231,7 @@ apspie_status apspie_ctx_create(int device, void *cuda_stream, apspie_ctx **out)
               cudaMalloc(&ctx->d_sticky_err, sizeof(int)) == cudaSuccess &&
               cudaMallocHost(&ctx->h_ctl, sizeof(TravCtl)) == cudaSuccess &&
               cudaMallocHost(&ctx->h_word, 64) == cudaSuccess &&
+              cudaMallocHost(&ctx->h_limit, 64) == cudaSuccess &&
               cudaMemset(ctx->d_sticky_err, 0, sizeof(int)) == cudaSuccess &&
               cudaMemset(ctx->d_ctl, 0, sizeof(TravCtl)) == cudaSuccess;
     if (!ok) {
@@ -236,6 +253,7 @@ void apspie_ctx_destroy(apspie_ctx *ctx) {
     if (ctx->d_sticky_err) cudaFree(ctx->d_sticky_err);
     if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
     if (ctx->h_word) cudaFreeHost(ctx->h_word);
+    if (ctx->h_limit) cudaFreeHost(ctx->h_limit);
     delete ctx;
 }
 
@@ -302,6 +320,37 @@ apspie_status apspie_ctx_set_max_grid(apspie_ctx *ctx, int32_t max_blocks) {
     if (!ctx || max_blocks < 0) return APSPIE_ERR_INVALID_ARG;
     ctx->max_grid = max_blocks;
     return APSPIE_OK;
+}
+
+apspie_status apspie_ctx_set_wait_limit(apspie_ctx *ctx, int64_t ns) {
+    if (!ctx) return APSPIE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    // calls already enqueued may still read the pinned copy
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_error(ctx, e, "set_wait_limit");
+    ctx->wait_limit_ns = ns > 0 ? static_cast<unsigned long long>(ns) : 0ull;
+    *ctx->h_limit = ctx->wait_limit_ns;
+    return APSPIE_OK;
+}
+
+apspie_status apspie_grid_barrier_check(apspie_ctx *ctx, int32_t rounds, int32_t absent_block, int32_t *grid) {
+    if (!ctx || rounds < 0) return APSPIE_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    apspie_status st = reset_ctl(ctx);
+    if (st != APSPIE_OK) return st;
+    int g = 0;
+    void *args[4];
+    int *sticky = ctx->d_sticky_err;
+    TravCtl *ctl = ctx->d_ctl;
+    args[0] = &ctl;
+    args[1] = &sticky;
+    args[2] = &rounds;
+    args[3] = &absent_block;
+    st = launch_persistent(ctx, reinterpret_cast<const void *>(barrier_check_kernel), 256, args, 1LL << 40, &g);
+    if (st != APSPIE_OK) return st;
+    if (grid) *grid = g;
+    apspie_run_stats rs;  // reads the control block back: the device's status
+    return finish_call(ctx, &rs, "apspie_grid_barrier_check");
 }
 
 apspie_status apspie_ctx_timeline(const apspie_ctx *ctx, int32_t *sites, int64_t *ns, int32_t cap,

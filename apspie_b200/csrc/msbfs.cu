@@ -489,8 +489,8 @@ apspie_status bfs_batch_impl(apspie_ctx *ctx, const apspie_csr *A, const int32_t
         } else {
             e = cudaMemsetAsync(a.out, 0xff, static_cast<size_t>(nq) * m * sizeof(int32_t), ctx->stream);
         }
-        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(TravCtl), ctx->stream);
         if (e != cudaSuccess) return cuda_error(ctx, e, "apspie_bfs_batch reset");
+        if ((st = reset_ctl(ctx)) != APSPIE_OK) return st;
         const void *fn = Wp == 1 ? msbfs_fn<1>() : Wp == 2 ? msbfs_fn<2>() : Wp == 4 ? msbfs_fn<4>()
                          : Wp == 8 ? msbfs_fn<8>() : msbfs_fn<16>();
         void *args[] = {&a};

@@ -328,8 +328,8 @@ extern "C" apspie_status apspie_sssp_batch(apspie_ctx *ctx, const apspie_csr *A,
         a.ctl = ctx->d_ctl;
         a.sticky = ctx->d_sticky_err;
         cudaError_t e = cudaMemsetAsync(a.lab, 0xff, mw * 32 * sizeof(unsigned), ctx->stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(TravCtl), ctx->stream);
         if (e != cudaSuccess) return cuda_error(ctx, e, "apspie_sssp_batch reset");
+        if ((st = reset_ctl(ctx)) != APSPIE_OK) return st;
         void *args[] = {&a};
         st = launch_persistent(ctx, reinterpret_cast<const void *>(sssp_batch_kernel), kSbBlock, args, 1LL << 40);
         if (st != APSPIE_OK) return st;

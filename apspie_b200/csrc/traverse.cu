@@ -1038,10 +1038,6 @@ apspie_status prepare_square(apspie_ctx *ctx, const apspie_csr *A, const char *w
     return APSPIE_OK;
 }
 
-apspie_status reset_ctl(apspie_ctx *ctx) {
-    cudaError_t e = cudaMemsetAsync(ctx->d_ctl, 0, sizeof(TravCtl), ctx->stream);
-    return e == cudaSuccess ? APSPIE_OK : cuda_error(ctx, e, "control reset");
-}
 
 }  // namespace
 

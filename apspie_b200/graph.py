@@ -293,6 +293,16 @@ class Context:
     def set_max_grid(self, blocks: int) -> None:
         self._check(L.lib().apspie_ctx_set_max_grid(self.handle, blocks), "set_max_grid")
 
+    def set_wait_limit(self, ns: int) -> None:
+        self._check(L.lib().apspie_ctx_set_wait_limit(self.handle, int(ns)), "set_wait_limit")
+
+    def grid_barrier_check(self, rounds: int, absent_block: int = -1) -> int:
+        """Runs the grid-barrier health check; returns the grid size (raises on a timeout)."""
+        g = ctypes.c_int32(0)
+        self._check(L.lib().apspie_grid_barrier_check(self.handle, rounds, absent_block, ctypes.byref(g)),
+                    "grid_barrier_check")
+        return g.value
+
     def reserve(self, m: int, nnz: int) -> None:
         self._check(L.lib().apspie_ctx_reserve(self.handle, m, nnz), "reserve")
 

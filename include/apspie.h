@@ -124,6 +124,19 @@ apspie_status apspie_ctx_set_batch_push_frac(apspie_ctx *ctx, float frac);
 /* Caps the number of co-resident blocks of the persistent traversal kernels
  * (0 = as many as fit). */
 apspie_status apspie_ctx_set_max_grid(apspie_ctx *ctx, int32_t max_blocks);
+/* Bound of every device-side wait of this context's persistent kernels (the grid barrier
+ * between their phases), in nanoseconds; ns <= 0 restores the default of 4 s. A wait that
+ * runs out raises APSPIE_ERR_TIMEOUT, every block of the launch leaves, and the call (or
+ * the next apspie_ctx_synchronize) returns that status; the context stays usable. No
+ * reference counterpart (the reference synchronises on the host every level). */
+apspie_status apspie_ctx_set_wait_limit(apspie_ctx *ctx, int64_t ns);
+/* Health check of the persistent-kernel machinery on this context's device and stream:
+ * one cooperative grid as large as the traversal kernels use passes `rounds` grid
+ * barriers. With absent_block >= 0 that block leaves before its first arrival, so the
+ * others' wait runs out after the context's wait limit and the call returns
+ * APSPIE_ERR_TIMEOUT -- the timeout path exercised without disturbing the GPU. *grid (may
+ * be NULL) receives the number of blocks launched. Synchronous. */
+apspie_status apspie_grid_barrier_check(apspie_ctx *ctx, int32_t rounds, int32_t absent_block, int32_t *grid);
 /* Phase timeline of the last traversal call made with a stats pointer: for each grid
  * barrier block 0 passed (up to 128), the barrier's site code and the nanoseconds since the
  * kernel started (globaltimer). Site 0 is the kernel start. */
