@@ -86,7 +86,8 @@ class TuneParams(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, c_int64) for n in ("submitted", "completed", "failed", "launches", "batched_queries",
-                                        "max_batch_seen", "deferred", "peak_bytes", "resident_bytes")]
+                                        "max_batch_seen", "deferred", "peak_bytes", "resident_bytes",
+                                        "joined_running", "trivial")]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -159,6 +160,8 @@ SIGNATURES = {
     "apspie_server_start": (c_int, [c_void_p]),
     "apspie_server_submit": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, POINTER(ctypes.c_uint64)]),
     "apspie_server_wait": (c_int, [c_void_p, ctypes.c_uint64, c_int32, POINTER(c_double)]),
+    "apspie_server_take_completed": (c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
+                                             POINTER(c_int32)]),
     "apspie_server_poll": (c_int, [c_void_p, ctypes.c_uint64, POINTER(c_int32)]),
     "apspie_server_get_stats": (c_int, [c_void_p, POINTER(ServerStats)]),
     "apspie_server_destroy": (None, [c_void_p]),

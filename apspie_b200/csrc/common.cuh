@@ -150,6 +150,22 @@ size_t bfs_batch_scratch_need(int m, int nq);  // apspie_bfs_batch (nq <= 512 pe
 // h_rows is given, else into the query-major d_depths
 apspie_status bfs_batch_impl(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_sources, int32_t num_sources,
                              int32_t depth_cap, int32_t *d_depths, int32_t *const *h_rows, apspie_run_stats *stats);
+// The server's continuous BFS engine (msbfs.cu): a persistent batched BFS with 32 * W
+// query slots that takes requests from a host-mapped ring at every level and posts each
+// query's completion as soon as its frontier dies.
+}  // namespace apspie
+struct BfsEngine;
+namespace apspie {
+size_t bfs_engine_scratch_need(int m, int W);
+int bfs_engine_words(int slots);  // W for at least `slots` query slots (32..512)
+apspie_status bfs_engine_create(BfsEngine **out);
+void bfs_engine_destroy(BfsEngine *e);
+bool bfs_engine_post(BfsEngine *e, int source, int *row, unsigned long long id);
+int bfs_engine_completions(BfsEngine *e, unsigned long long *ids, int cap);
+unsigned long long bfs_engine_waiting(const BfsEngine *e);
+void bfs_engine_set_accept(BfsEngine *e, int on);
+std::vector<unsigned long long> bfs_engine_take_back(BfsEngine *e);  // untaken ring entries (launch ended)
+apspie_status bfs_engine_launch(apspie_ctx *ctx, const apspie_csr *A, int W, BfsEngine *e);
 size_t sssp_batch_scratch_need(int m, int nq);  // apspie_sssp_batch (nq <= 512 per launch)
 // apspie_sssp_batch in query groups (each group of blocks runs single-source SSSPs)
 size_t sssp_group_scratch_need(int m, int groups);

@@ -615,6 +615,17 @@ class Server:
         L.check(L.lib().apspie_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(lat)), None, "server_wait")
         return lat.value
 
+    def take_completed(self, cap: int = 1024, timeout_ms: int = 600000):
+        """[(ticket, status, latency_ms)] of requests completed since the last call (>= 1)."""
+        t = np.zeros(cap, dtype=np.uint64)
+        stv = np.zeros(cap, dtype=np.int32)
+        lat = np.zeros(cap, dtype=np.float64)
+        n = ctypes.c_int32()
+        L.check(L.lib().apspie_server_take_completed(self.handle, timeout_ms, cap, t.ctypes.data, stv.ctypes.data,
+                                                     lat.ctypes.data, ctypes.byref(n)), None, "server_take_completed")
+        k = n.value
+        return list(zip(t[:k].tolist(), stv[:k].tolist(), lat[:k].tolist()))
+
     def done(self, ticket: int) -> bool:
         d = ctypes.c_int32()
         L.check(L.lib().apspie_server_poll(self.handle, ticket, ctypes.byref(d)), None, "server_poll")

@@ -3,11 +3,12 @@
  *
  * No reference counterpart: the reference answers one query per process run
  * (test/bfs/run.sh, test/sssp/run.sh, test/mis/run.sh). The server keeps several graphs on
- * one GPU, admits BFS / SSSP / MIS requests against a device-memory budget and folds
- * requests that wait on the same graph into one launch (BFS: apspie_bfs_batch; SSSP:
- * one apspie_sssp per request, or apspie_sssp_batch when folding is enabled; MIS: one
- * apspie_mis shared by all waiting requests), on several
- * execution slots whose launches overlap on the device. Each answer is written by the same
+ * one GPU, admits BFS / SSSP / MIS requests against a device-memory budget and runs them
+ * on several execution slots whose launches overlap on the device. BFS requests on a graph
+ * join a running batched-BFS launch (the graph's engine) at its next level boundary and
+ * complete individually as soon as their own search ends; SSSP requests fold into
+ * apspie_sssp_batch or run apspie_sssp each; MIS requests share one apspie_mis. Sources
+ * without edges are answered by a small fill kernel. Each answer is written by the same
  * kernels as the plain entry points, so it is identical alone or in a mix.
  */
 #ifndef APSPIE_SERVER_H
@@ -40,11 +41,13 @@ typedef struct apspie_server_stats {
     int64_t deferred;         /* admission attempts postponed by the memory budget */
     int64_t peak_bytes;       /* largest device footprint admitted */
     int64_t resident_bytes;   /* graphs + per-slot reserved scratch */
+    int64_t joined_running;   /* BFS requests posted into an engine launch already on the GPU */
+    int64_t trivial;          /* BFS / SSSP requests whose source has no edges (no traversal) */
 } apspie_server_stats;
 
 /* device: GPU ordinal; memory_budget_bytes: device bytes the server may hold (graphs,
- * scratch, batch staging); num_slots: concurrent launches (1..16); max_batch: BFS
- * requests per launch. */
+ * scratch, batch staging); num_slots: concurrent launches (1..16); max_batch: query slots
+ * of a BFS engine and requests per SSSP batch (at most 512). */
 apspie_status apspie_server_create(int device, int64_t memory_budget_bytes, int32_t num_slots,
                                    int32_t max_batch, apspie_server **out);
 /* Uploads a graph (host CSR; int32 weights enable SSSP). symmetric != 0 marks it
@@ -74,6 +77,13 @@ apspie_status apspie_server_submit(apspie_server *s, int32_t graph_id, int32_t k
  * the latency from submit to completion in *latency_ms. A ticket can be waited once. */
 apspie_status apspie_server_wait(apspie_server *s, uint64_t ticket, int32_t timeout_ms,
                                  double *latency_ms);
+/* Completed requests in completion order, for callers that keep many in flight: blocks
+ * until at least one request not yet waited for has completed (or timeout_ms passes:
+ * APSPIE_ERR_TIMEOUT; < 0 waits without limit), then reports up to cap of them
+ * (tickets[i], statuses[i], latencies_ms[i]; the last two may be NULL) and *count. A ticket
+ * reported here cannot be waited for again. */
+apspie_status apspie_server_take_completed(apspie_server *s, int32_t timeout_ms, int32_t cap, uint64_t *tickets,
+                                           int32_t *statuses, double *latencies_ms, int32_t *count);
 /* Non-blocking completion test. */
 apspie_status apspie_server_poll(apspie_server *s, uint64_t ticket, int32_t *done);
 apspie_status apspie_server_get_stats(apspie_server *s, apspie_server_stats *out);

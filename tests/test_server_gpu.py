@@ -87,9 +87,10 @@ def test_server_budget_enforced(graphs):
 
 def test_server_tight_budget_shrinks_batches_but_answers_stay_exact(ctx, graphs):
     g = graphs[2]
-    # A one-query server reserves the graph plus the arena of a one-word (<= 32 query)
-    # batch. 64 KB more than that lets the tight server's arena grow to a one-word batch
-    # but not to the two-word arena (12 bytes per vertex more) that 64 sources would need.
+    # A one-query server reserves the graph plus the arena of a BFS engine with one word
+    # (32 query slots). 64 KB more than that lets the tight server's arena grow to a
+    # one-word engine but not to the two-word one (12 bytes per vertex more) that 64 waiting
+    # sources would ask for; the engine then serves them 32 at a time.
     probe = ap.Server(0, budget_bytes=4 << 30, slots=1, max_batch=1)
     probe.add_graph(g)
     probe.start()
@@ -126,4 +127,55 @@ def test_server_rejects_bad_requests(graphs):
         srv.submit(gid, L.QUERY_SSSP, 0, o)  # no weights on this graph
     with pytest.raises(ap.ApspieError):
         srv.submit(gid + 1, L.QUERY_BFS, 0, o)
+    srv.close()
+
+
+def test_server_bfs_arrivals_join_the_running_engine(ctx):
+    """Bursts of BFS requests arrive while the graph's engine is on the GPU: they are posted
+    into the running launch (joined_running > 0) and every answer equals the plain path's,
+    including sources without edges (answered without a traversal)."""
+    import time
+
+    g = ap.gen_rmat(16, 16, 5, 3)
+    srv = ap.Server(0, budget_bytes=8 << 30, slots=1, max_batch=256)
+    gid = srv.add_graph(g)
+    srv.start()
+    rng = np.random.default_rng(11)
+    srcs = [int(x) for x in rng.integers(0, g.m, 600)]
+    outs, tickets = [], []
+    for burst in range(12):
+        for s in srcs[burst * 50:(burst + 1) * 50]:
+            o = _out(g, L.QUERY_BFS)
+            outs.append(o)
+            tickets.append(srv.submit(gid, L.QUERY_BFS, s, o))
+        time.sleep(0.0005)
+    done = {}
+    while len(done) < len(tickets):
+        for t, status, lat in srv.take_completed():
+            assert status == 0
+            done[t] = lat
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == 600 and st["failed"] == 0
+    assert st["joined_running"] > 0
+    assert st["trivial"] == sum(1 for s in srcs if g.row_ptr[s + 1] == g.row_ptr[s])
+    dg = ap.DeviceGraph(g)
+    for s, o in zip(srcs, outs):
+        np.testing.assert_array_equal(o.cpu().numpy(), ctx.bfs(dg, s).cpu().numpy(), err_msg=str(s))
+
+
+def test_server_take_completed_reports_each_request_once(ctx, graphs):
+    g = graphs[1]
+    srv = ap.Server(0, budget_bytes=2 << 30, slots=2, max_batch=64)
+    gid = srv.add_graph(g)
+    srv.start()
+    outs = [_out(g, k) for k in (L.QUERY_BFS, L.QUERY_SSSP, L.QUERY_MIS) for _ in range(20)]
+    kinds = [k for k in (L.QUERY_BFS, L.QUERY_SSSP, L.QUERY_MIS) for _ in range(20)]
+    tickets = [srv.submit(gid, k, (7 * i) % g.m, o) for i, (k, o) in enumerate(zip(kinds, outs))]
+    seen = []
+    while len(seen) < len(tickets):
+        seen += [t for t, status, _ in srv.take_completed(cap=7) if status == 0]
+    assert sorted(seen) == sorted(tickets)
+    with pytest.raises(ap.ApspieError):
+        srv.wait(tickets[0], timeout_ms=10)  # already reported
     srv.close()
