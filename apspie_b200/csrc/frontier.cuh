@@ -56,6 +56,7 @@ struct ExpandSmem {
     int base[kMaxGrid + 1];  // exclusive prefix of chunk totals
     int tsplit[BATCH + 1];   // merge-path split of each warp tile of the current batch
     int next_tile;           // tiles of the batch handed out so far (warps take them in turn)
+    int claim_base;          // first tile of the chunk this block claimed (grid-wide claiming)
     int scan_tmp[33];
     Warp w[NWARP];
 };
@@ -158,11 +159,15 @@ __device__ __forceinline__ int frontier_merge_path(long long diag, int nf, int E
 // entries k[]); post(ne, ws) runs after the tile's edges (per-entry flushes). All three
 // are called by every lane of the warp, so they may use warp collectives. DYN: warps claim
 // the tiles of their block's batch in turn (else tile i goes to warp i % NWARP).
+// claim == nullptr: every block owns a contiguous run of tiles. Otherwise blocks claim
+// chunks of 2 * NWARP consecutive tiles from the grid-wide counter *claim (zero when the
+// phase starts) until none is left, so that blocks whose tiles were cheap take more and
+// no block idles at the phase's end while another still has a long run to go.
 template <int BLOCK, int VT, bool EXTRA, bool DYN = true, class Load, class Op, class Post>
 __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__restrict__ loc_off,
                                                 const int *__restrict__ rs,
                                                 ExpandSmem<BLOCK, VT, EXTRA> &sm, Load load, Op op,
-                                                Post post, VGrid vg = hw_grid()) {
+                                                Post post, VGrid vg = hw_grid(), int *claim = nullptr) {
     using S = ExpandSmem<BLOCK, VT, EXTRA>;
     constexpr int WT = S::WT;
     constexpr int NWARP = S::NWARP;
@@ -171,14 +176,73 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
     const int C = (nf + G - 1) / G;
     const long long total = static_cast<long long>(nf) + E;
     const long long ntiles = (total + WT - 1) / WT;
-    const long long per = (ntiles + G - 1) / G;
-    const long long t_begin = static_cast<long long>(vg.id) * per;
-    const long long t_end = t_begin + per < ntiles ? t_begin + per : ntiles;
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     typename S::Warp &ws = sm.w[wid];
-    for (long long tb = t_begin; tb < t_end; tb += BATCH) {
-        const long long te = tb + BATCH < t_end ? tb + BATCH : t_end;
+    // one warp tile: stage its entries, label its edge slots, run the operation
+    auto run_tile = [&](long long tile, long long tb) {
+        const long long d0 = tile * WT;
+        const long long d1 = d0 + WT < total ? d0 + WT : total;
+        const int a0 = sm.tsplit[tile - tb];
+        const int a1 = sm.tsplit[tile - tb + 1];
+        const int e0 = static_cast<int>(d0 - a0);
+        const int e1 = static_cast<int>(d1 - a1);
+        const int jb = a0 > 0 ? a0 - 1 : 0;
+        const int ne = a1 - jb;
+        for (int k = lane; k < ne; k += 32) {
+            const int j = jb + k;
+            ws.off[k] = sm.base[j / C] + __ldcg(loc_off + j);
+            ws.rs[k] = __ldcg(rs + j);
+            load(j, k, ws);
+        }
+        __syncwarp();
+        const int tcount = static_cast<int>(d1 - d0);
+        const int diag = lane * VT;
+        if (diag < tcount) {
+            const int acount = a1 - a0, bcount = e1 - e0;
+            int lo = diag - bcount > 0 ? diag - bcount : 0;
+            int hi = diag < acount ? diag : acount;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (ws.off[a0 + mid - jb] <= e0 + diag - 1 - mid)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            int ja = a0 + lo, eb = e0 + diag - lo;
+            int cur = ja - 1 - jb;
+            const int end = diag + VT < tcount ? diag + VT : tcount;
+            for (int it = diag; it < end; ++it) {
+                if (ja < a1 && ws.off[ja - jb] <= eb) {
+                    cur = ja - jb;
+                    ++ja;
+                } else {
+                    ws.seg[eb - e0] = cur;
+                    ++eb;
+                }
+            }
+        }
+        __syncwarp();
+        const int ned = e1 - e0;
+        bool valid[VT];
+        int kk[VT], idx[VT];
+#pragma unroll
+        for (int r = 0; r < VT; ++r) {
+            const int el = r * 32 + lane;
+            valid[r] = el < ned;
+            kk[r] = 0;
+            idx[r] = 0;
+            if (valid[r]) {
+                kk[r] = ws.seg[el];
+                idx[r] = ws.rs[kk[r]] + (e0 + el - ws.off[kk[r]]);
+            }
+        }
+        op(valid, kk, idx, ws);
+        __syncwarp();
+        post(ne, ws);
+    };
+    // the tiles [tb, te) of one batch: split points found together, then the warps
+    auto run_batch = [&](long long tb, long long te) {
         for (int s = threadIdx.x; s <= te - tb; s += BLOCK) {
             long long d = (tb + s) * WT;
             if (d > total) d = total;
@@ -189,65 +253,7 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
         // a warp that finishes its tile takes the next unclaimed one, so tiles of uneven
         // cost (atomics, queue flushes) do not leave warps idle at the batch's barrier
         for (long long tile = tb + wid; tile < te;) {
-            const long long d0 = tile * WT;
-            const long long d1 = d0 + WT < total ? d0 + WT : total;
-            const int a0 = sm.tsplit[tile - tb];
-            const int a1 = sm.tsplit[tile - tb + 1];
-            const int e0 = static_cast<int>(d0 - a0);
-            const int e1 = static_cast<int>(d1 - a1);
-            const int jb = a0 > 0 ? a0 - 1 : 0;
-            const int ne = a1 - jb;
-            for (int k = lane; k < ne; k += 32) {
-                const int j = jb + k;
-                ws.off[k] = sm.base[j / C] + __ldcg(loc_off + j);
-                ws.rs[k] = __ldcg(rs + j);
-                load(j, k, ws);
-            }
-            __syncwarp();
-            const int tcount = static_cast<int>(d1 - d0);
-            const int diag = lane * VT;
-            if (diag < tcount) {
-                const int acount = a1 - a0, bcount = e1 - e0;
-                int lo = diag - bcount > 0 ? diag - bcount : 0;
-                int hi = diag < acount ? diag : acount;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (ws.off[a0 + mid - jb] <= e0 + diag - 1 - mid)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
-                }
-                int ja = a0 + lo, eb = e0 + diag - lo;
-                int cur = ja - 1 - jb;
-                const int end = diag + VT < tcount ? diag + VT : tcount;
-                for (int it = diag; it < end; ++it) {
-                    if (ja < a1 && ws.off[ja - jb] <= eb) {
-                        cur = ja - jb;
-                        ++ja;
-                    } else {
-                        ws.seg[eb - e0] = cur;
-                        ++eb;
-                    }
-                }
-            }
-            __syncwarp();
-            const int ned = e1 - e0;
-            bool valid[VT];
-            int kk[VT], idx[VT];
-#pragma unroll
-            for (int r = 0; r < VT; ++r) {
-                const int el = r * 32 + lane;
-                valid[r] = el < ned;
-                kk[r] = 0;
-                idx[r] = 0;
-                if (valid[r]) {
-                    kk[r] = ws.seg[el];
-                    idx[r] = ws.rs[kk[r]] + (e0 + el - ws.off[kk[r]]);
-                }
-            }
-            op(valid, kk, idx, ws);
-            __syncwarp();
-            post(ne, ws);
+            run_tile(tile, tb);
             if (DYN) {
                 int nt = 0;
                 if (lane == 0) nt = atomicAdd(&sm.next_tile, 1);
@@ -258,6 +264,23 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
             __syncwarp();
         }
         __syncthreads();
+    };
+    if (claim == nullptr) {
+        const long long per = (ntiles + G - 1) / G;
+        const long long t_begin = static_cast<long long>(vg.id) * per;
+        const long long t_end = t_begin + per < ntiles ? t_begin + per : ntiles;
+        for (long long tb = t_begin; tb < t_end; tb += BATCH)
+            run_batch(tb, tb + BATCH < t_end ? tb + BATCH : t_end);
+    } else {
+        constexpr int CH = 2 * NWARP;
+        for (;;) {
+            if (threadIdx.x == 0) sm.claim_base = atomicAdd(claim, CH);
+            __syncthreads();
+            const long long tb = sm.claim_base;
+            if (tb >= ntiles) break;
+            run_batch(tb, tb + CH < ntiles ? tb + CH : ntiles);  // ends with __syncthreads
+        }
+        __syncthreads();  // every thread has read claim_base before it is reused
     }
 }
 

@@ -30,6 +30,12 @@ namespace {
 #ifndef APSPIE_SSSP_PREREAD
 #define APSPIE_SSSP_PREREAD 1
 #endif
+#ifndef APSPIE_SSSP_CLAIM
+#define APSPIE_SSSP_CLAIM 0  // 1: blocks claim expansion tiles from a grid-wide counter
+#endif
+#ifndef APSPIE_TRAV_CLAIM
+#define APSPIE_TRAV_CLAIM 0  // the same for the BFS push and MIS expansions
+#endif
 
 
 constexpr int kBlock = 256;
@@ -168,7 +174,10 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
                                      atomicOr(fbc + (v >> 5), 1u << (v & 31));
                                      return deg;
                                  });
-        if (gtid == 0) *qlen_next = 0;
+        if (gtid == 0) {
+            *qlen_next = 0;
+            a.ctl->claim = 0;
+        }
         if (!grid_barrier(a.ctl, a.sticky, kSiteBfs + 1)) return;
 
         const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
@@ -215,7 +224,7 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
                         wq.push(fresh[r], v[r]);
                     }
                 },
-                NoPost());
+                NoPost(), hw_grid(), APSPIE_TRAV_CLAIM ? &a.ctl->claim : nullptr);
             wq.flush();
         } else {
             ++npull;
@@ -547,6 +556,7 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
             }
             if (threadIdx.x == 0) a.buf.chunk_sum[vg.id] = carry;
         }
+        if (APSPIE_SSSP_CLAIM && gtid == 0) a.ctl->claim = 0;
         if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarA, vg)) return;
         // every block has read this queue's length, base and histogram: reset them for the
         // iteration that fills this queue next
@@ -662,7 +672,7 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
                     wf.push(far[r], v[r]);
                 }
             },
-            NoPost(), vg);
+            NoPost(), vg, APSPIE_SSSP_CLAIM ? &a.ctl->claim : nullptr);
         wn.flush();
         wf.flush();
         if (banded) {
@@ -907,7 +917,10 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
             }
             if (threadIdx.x == 0) a.buf.chunk_sum[blockIdx.x] = carry;
         }
-        if (gtid == 0) *qlen_next = 0;
+        if (gtid == 0) {
+            *qlen_next = 0;
+            a.ctl->claim = 0;
+        }
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 1)) return;
 
         // phase B: pushes and scans
@@ -951,7 +964,8 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                     const int f = ws.flag[k];
                     if (f != kInf) atomicMin(first + ws.aux[k], f);
                 }
-            });
+            },
+            hw_grid(), APSPIE_TRAV_CLAIM ? &a.ctl->claim : nullptr);
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 2)) return;
 
         // phase C: decisions

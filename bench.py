@@ -249,7 +249,9 @@ def main_ours(args, ws, rank, local):
     if args.only_extra:
         # one extra leg alone (for profiling a kernel without the rest of the run)
         ctx = ap.Context(local)
-        if args.only_extra == "spgemm_tc":
+        if args.only_extra == "traversal":
+            res = extras_traversal(ctx, args, ws, local)
+        elif args.only_extra == "spgemm_tc":
             res = extras_spgemm_tc(ctx, args, ws, local)
         elif args.only_extra == "build":
             res = extras_build(ctx, args, ws, local)
@@ -370,7 +372,23 @@ def cpu_baseline(g, src, comp_edges):
 
 
 def extras(ctx, args, ws, local):
-    """BFS on R-MAT scale 14 (seed 1) and MIS on R-MAT scale 20 (seed 2), same timing rules."""
+    """Every extra leg: traversal kernels, SpGEMM / TC, device construction, batched
+    traversal and serving."""
+    import apspie_b200 as ap
+
+    res = extras_traversal(ctx, args, ws, local)
+    res.update(extras_spgemm_tc(ctx, args, ws, local))
+    res.update(extras_build(ctx, args, ws, local))
+    g22 = ap.gen_rmat(22, 16, 1, 3)  # weights for the serving leg; BFS ignores them
+    res.update(extras_batched(ctx, args, ws, local, g22))
+    if ws == 1:
+        res.update(extras_serving(ctx, args, local, g22))
+    return res
+
+
+def extras_traversal(ctx, args, ws, local):
+    """BFS on R-MAT scale 14 (seed 1), MIS and BFS on R-MAT scale 20 (seed 2), same timing
+    rules; MIS and BFS at scale 20 with their algorithmic-bytes roofline."""
     import torch
 
     import apspie_b200 as ap
@@ -408,9 +426,11 @@ def extras(ctx, args, ws, local):
     steps = max(5, min(args.steps, 20))
     tot, _ = time_steps(ctx.stream, lambda: ctx.mis_into(d20, prio, mem), steps)
     ms = max_over_ranks(ws, tot / steps)
+    peak, peak_kind = hbm_peak()
     alg = 4 * g20.nnz + 13 * g20.m
     res["mis_rmat20"] = {"ms": ms, "rounds": st["iterations"], "set_size": st["vertices_reached"],
                          "edges_scanned": st["edges_expanded"], "alg_GBps": alg / (ms * 1e-3) / 1e9,
+                         "frac": alg / (ms * 1e-3) / 1e9 / peak, "peak": f"{peak} GB/s ({peak_kind})",
                          "exact": bool(np.array_equal(mem.cpu().numpy(), oracle.mis_greedy(g20.row_ptr, g20.col_ind, pr)))}
     # BFS at scale 20 for the roofline of the BFS kernel on an HBM-sized graph
     s20 = ap.max_degree_vertex(g20)
@@ -421,16 +441,13 @@ def extras(ctx, args, ws, local):
     steps = max(args.steps, 20)
     tot, _ = time_steps(ctx.stream, lambda: ctx.bfs_into(d20, s20, o20), steps)
     ms = max_over_ranks(ws, tot / steps)
+    alg = 4 * st["edges_component"] + 8 * st["vertices_reached"] + 4 * g20.m
     res["bfs_rmat20"] = {"GTEPS": ws * st["edges_component"] / (ms * 1e-3) / 1e9, "ms": ms,
                          "levels": st["iterations"], "push_levels": st["push_iterations"],
-                         "pull_levels": st["pull_iterations"]}
+                         "pull_levels": st["pull_iterations"], "alg_GBps": alg / (ms * 1e-3) / 1e9,
+                         "frac": alg / (ms * 1e-3) / 1e9 / peak,
+                         "exact": bool(np.array_equal(o20.cpu().numpy(), oracle.bfs(g20.row_ptr, g20.col_ind, s20)))}
     del d20, o20, mem, prio
-    res.update(extras_spgemm_tc(ctx, args, ws, local))
-    res.update(extras_build(ctx, args, ws, local))
-    g22 = ap.gen_rmat(22, 16, 1, 3)  # weights for the serving leg; BFS ignores them
-    res.update(extras_batched(ctx, args, ws, local, g22))
-    if ws == 1:
-        res.update(extras_serving(ctx, args, local, g22))
     return res
 
 
@@ -536,17 +553,28 @@ def extras_batched(ctx, args, ws, local, g):
     tot, _ = time_steps(ctx.stream, lambda: [ctx.bfs_into(dg, int(x), one) for x in srcs[:64]], 1)
     plain_ms = max_over_ranks(ws, tot / 64)
     res = {"plain_bfs_rmat22": {"ms_per_query": plain_ms, "queries_per_s": ws * 1e3 / plain_ms}}
+    # every batched row is compared with the plain path's answer for its source (row hashes),
+    # and row 0 with the oracle
+    ref = RowHasher(g.m, 512, dev)
+    for q, x in enumerate(srcs):
+        ctx.bfs_into(dg, int(x), one)
+        ref.put(q, one)
+    ref_h = ref.result()
     for nq in (32, 128, 512):
         s = torch.from_numpy(srcs[:nq]).to(dev)
         out = torch.empty((nq, g.m), dtype=torch.int32, device=dev)
         ctx.bfs_batch_into(dg, s, out)
         tot, per = time_steps(ctx.stream, lambda: ctx.bfs_batch_into(dg, s, out), 3)
         ms = max_over_ranks(ws, tot / 3)
-        exact = all(np.array_equal(out[q].cpu().numpy(), oracle.bfs(g.row_ptr, g.col_ind, int(srcs[q])))
-                    for q in (0, nq - 1))
+        h = RowHasher(g.m, nq, dev)
+        h.coef = ref.coef
+        for q in range(nq):
+            h.put(q, out[q])
+        same = int((h.result() == ref_h[:nq]).sum())
+        exact = same == nq and np.array_equal(out[0].cpu().numpy(), oracle.bfs(g.row_ptr, g.col_ind, int(srcs[0])))
         res[f"batched_bfs_rmat22_B{nq}"] = {"ms_per_batch": ms, "queries_per_s": ws * nq * 1e3 / ms,
-                                            "x_plain": plain_ms * nq / ms, "p99_ms": float(np.percentile(per, 99)),
-                                            "exact_checked_rows": bool(exact)}
+                                            "x_plain": plain_ms * nq / ms, "rows_checked": nq,
+                                            "rows_equal_plain": same, "exact": bool(exact)}
         del out
     # SSSP: the plain loop over 16 sources (each query takes milliseconds), then the batches
     for x in srcs[:2]:
@@ -554,6 +582,11 @@ def extras_batched(ctx, args, ws, local, g):
     tot, _ = time_steps(ctx.stream, lambda: [ctx.sssp_into(dg, int(x), one) for x in srcs[:16]], 1)
     plain_ms = max_over_ranks(ws, tot / 16)
     res["plain_sssp_rmat22"] = {"ms_per_query": plain_ms, "queries_per_s": ws * 1e3 / plain_ms}
+    ref = RowHasher(g.m, 512, dev)
+    for q, x in enumerate(srcs):
+        ctx.sssp_into(dg, int(x), one)
+        ref.put(q, one)
+    ref_h = ref.result()
     for nq in (32, 128, 512):
         s = torch.from_numpy(srcs[:nq]).to(dev)
         out = torch.empty((nq, g.m), dtype=torch.int32, device=dev)
@@ -561,30 +594,62 @@ def extras_batched(ctx, args, ws, local, g):
         reps = 3 if nq < 512 else 1
         tot, per = time_steps(ctx.stream, lambda: ctx.sssp_batch_into(dg, s, out), reps)
         ms = max_over_ranks(ws, tot / reps)
-        # row 0 against the oracle, the last row against the single-source kernel
-        ctx.sssp_into(dg, int(srcs[nq - 1]), one)
-        exact = np.array_equal(out[0].cpu().numpy(), oracle.sssp(g.row_ptr, g.col_ind, g.val, int(srcs[0]))) \
-            and torch.equal(out[nq - 1], one)
+        h = RowHasher(g.m, nq, dev)
+        h.coef = ref.coef
+        for q in range(nq):
+            h.put(q, out[q])
+        same = int((h.result() == ref_h[:nq]).sum())
+        exact = same == nq and np.array_equal(out[0].cpu().numpy(),
+                                              oracle.sssp(g.row_ptr, g.col_ind, g.val, int(srcs[0])))
         res[f"batched_sssp_rmat22_B{nq}"] = {"ms_per_batch": ms, "queries_per_s": ws * nq * 1e3 / ms,
-                                             "x_plain": plain_ms * nq / ms, "exact_checked_rows": bool(exact)}
+                                             "x_plain": plain_ms * nq / ms, "rows_checked": nq,
+                                             "rows_equal_plain": same, "exact": bool(exact)}
         del out
     return res
 
 
-SERVE_QUERIES = 2000  # a bounded sample of the 100,000-query stream
+SERVE_QUERIES = 100_000  # the serving stream's full length
+SERVE_SLOTS = 2
+SERVE_MAX_BATCH = 512
+POOL_ROWS = 512  # output rows per graph a stream keeps in flight (int32 rows; MIS: 64)
+
+
+class RowHasher:
+    """A 64-bit linear hash of a result row, computed on the device without a host sync:
+    h = sum_i row[i] * c[i] (int32 products, int64 sum; exact, so order-independent) with
+    per-position coefficients drawn once. Equal rows give equal hashes; a differing row
+    collides only with probability about 2^-32."""
+
+    def __init__(self, m_max, n, dev):
+        import torch
+
+        g = torch.Generator(device="cpu").manual_seed(12345)
+        self.coef = torch.randint(-(1 << 31), (1 << 31) - 1, (m_max,), generator=g, dtype=torch.int64)
+        self.coef = self.coef.to(torch.int32).to(dev)
+        self.out = torch.zeros(n, dtype=torch.int64, device=dev)
+
+    def put(self, i, row):
+        import torch
+
+        c = self.coef[: row.shape[0]]
+        self.out[i] = torch.sum(row.to(torch.int32) * c, dtype=torch.int64)
+
+    def result(self):
+        return self.out.cpu().numpy()
 
 
 def serve_stream(graphs, n, rate_qps, seed=7):
     """The request stream: from mt19937(seed) words, per query a kind (70 % BFS, 25 % SSSP,
     5 % MIS), a graph (uniform), a source (uniform in that graph) and a Poisson arrival
-    (exponential gaps at rate_qps; rate 0 = all at t=0)."""
+    (exponential gaps at rate_qps; rate 0 = all at t=0). Kinds, graphs and sources do not
+    depend on the rate."""
     import apspie_b200 as ap
 
     u = ap.mt19937_u32(seed, 4 * n).astype(np.float64).reshape(n, 4)
     r = u[:, 0] % 100
     kinds = np.where(r < 70, 0, np.where(r < 95, 1, 2)).astype(int)
     which = (u[:, 1] % len(graphs)).astype(int)
-    srcs = [int(u[i, 2] % graphs[which[i]].m) for i in range(n)]
+    srcs = (u[:, 2] % np.array([g.m for g in graphs])[which]).astype(np.int64)
     if rate_qps > 0:
         gaps = -np.log1p(-u[:, 3] / 4294967296.0) / rate_qps
         arrive = np.cumsum(gaps) - gaps[0]
@@ -598,8 +663,10 @@ def _pct(lat):
             "p99.9_ms": float(np.percentile(lat, 99.9))}
 
 
-def serve_plain(ctx, dgs, prios, stream, dev):
-    """One query at a time through the plain entry points, FIFO in arrival order."""
+def serve_plain(ctx, dgs, prios, stream, dev, hasher=None):
+    """One query at a time through the plain entry points, FIFO in arrival order; latency
+    from arrival to completion. With a hasher, every answer's hash is recorded (on the
+    library's stream, after the latency is taken)."""
     import torch
 
     kinds, which, srcs, arrive = stream
@@ -607,7 +674,8 @@ def serve_plain(ctx, dgs, prios, stream, dev):
     mis_out = [torch.empty(d.m, dtype=torch.uint8, device=dev) for d in dgs]
     lat = np.zeros(len(kinds))
     t0 = time.perf_counter()
-    for i, (k, w, s) in enumerate(zip(kinds, which, srcs)):
+    for i in range(len(kinds)):
+        k, w, s = int(kinds[i]), int(which[i]), int(srcs[i])
         now = time.perf_counter() - t0
         if now < arrive[i]:
             time.sleep(arrive[i] - now)
@@ -619,19 +687,20 @@ def serve_plain(ctx, dgs, prios, stream, dev):
             ctx.mis_into(dgs[w], prios[w], mis_out[w])
         ctx.synchronize()
         lat[i] = (time.perf_counter() - t0 - arrive[i]) * 1e3
+        if hasher is not None:
+            with torch.cuda.stream(ctx.stream):
+                hasher.put(i, mis_out[w] if k == 2 else outs[w])
     total = time.perf_counter() - t0
+    torch.cuda.synchronize()
     return lat, total
 
 
-SERVE_SLOTS = 2  # measured best of 1, 2, 4, 8 on this mix
-SERVE_MAX_BATCH = 128  # measured: 128 keeps most of the batching gain at a tenth of the p99
-
-
-def serve_server(graphs, stream, dev, check=(), slots=None, max_batch=None):
-    """The same stream through apspie_server (4 slots, 40 GB budget); a waiter thread
-    collects completions while the main thread submits at the arrival times."""
-    import threading
-
+def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None):
+    """The same stream through apspie_server (40 GB budget): the main thread submits at the
+    arrival times from a pool of output rows per graph and, whenever a pool runs dry or
+    while it waits for the next arrival, takes completed requests in bulk, hashes their
+    rows on the device and returns the rows to the pools. Latency = server latency (submit
+    to completion) + how late the submit was after the arrival."""
     import torch
 
     import apspie_b200 as ap
@@ -641,102 +710,131 @@ def serve_server(graphs, stream, dev, check=(), slots=None, max_batch=None):
                     max_batch=max_batch or SERVE_MAX_BATCH)
     gids = [srv.add_graph(g) for g in graphs]
     srv.start()
-    # warm-up: one burst of every (graph, kind) before the clock starts
+    pools = [[torch.empty(g.m, dtype=torch.int32, device=dev) for _ in range(POOL_ROWS)] for g in graphs]
+    mpools = [[torch.empty(g.m, dtype=torch.uint8, device=dev) for _ in range(64)] for g in graphs]
+    # warm-up: a burst of every (graph, kind) before the clock starts
     warm = []
     for gi, g in enumerate(graphs):
         for kind in (0, 1, 2):
-            for k in range(8):
-                o = torch.empty(g.m, dtype=torch.uint8 if kind == 2 else torch.int32, device=dev)
-                warm.append((srv.submit(gids[gi], kind, (k * 7919) % g.m, o), o))
-    for t, _ in warm:
+            for k in range(16):
+                o = (mpools if kind == 2 else pools)[gi][k]
+                warm.append(srv.submit(gids[gi], kind, (k * 7919 + 1) % g.m, o))
+    for t in warm:
         srv.wait(t)
-    del warm
     n = len(kinds)
-    tickets = [None] * n
-    outs = [None] * n
+    owner = {}  # ticket -> (query index, row tensor, pool)
+    late = np.zeros(n)
     lat = np.zeros(n)
-    ready = threading.Semaphore(0)
-    keep = set(check)
+    hashed = []  # rows hashed since the last stream sync (returned to pools after it)
 
-    def waiter():
-        for i in range(n):
-            ready.acquire()
-            lat[i] = srv.wait(tickets[i])
-            if i not in keep:
-                outs[i] = None
+    def drain(block):
+        got = []
+        if owner:
+            try:
+                got = srv.take_completed(cap=4096, timeout_ms=-1 if block else 0)
+            except ap.ApspieError as e:
+                if e.name != "APSPIE_ERR_TIMEOUT":
+                    raise
+        for t, status, ms in got:
+            i, row, pool = owner.pop(t)
+            if status != 0:
+                raise RuntimeError(f"request {i} failed with status {status}")
+            lat[i] = ms + late[i]
+            hasher.put(i, row)
+            hashed.append((row, pool))
+        if hashed and (block or len(hashed) >= 256):
+            torch.cuda.current_stream().synchronize()
+            for row, pool in hashed:
+                pool.append(row)
+            hashed.clear()
+        return len(got)
 
-    th = threading.Thread(target=waiter)
-    th.start()
     t0 = time.perf_counter()
     for i in range(n):
+        k, w, s = int(kinds[i]), int(which[i]), int(srcs[i])
+        while time.perf_counter() - t0 < arrive[i]:
+            if drain(False) == 0:
+                time.sleep(min(2e-4, max(0.0, arrive[i] - (time.perf_counter() - t0))))
+        pool = mpools[w] if k == 2 else pools[w]
+        while not pool:
+            drain(True)
+        row = pool.pop()
         now = time.perf_counter() - t0
-        if now < arrive[i]:
-            time.sleep(arrive[i] - now)
-        g = graphs[which[i]]
-        outs[i] = torch.empty(g.m, dtype=torch.uint8 if kinds[i] == 2 else torch.int32, device=dev)
-        tickets[i] = srv.submit(gids[which[i]], int(kinds[i]), srcs[i], outs[i])
-        ready.release()
-    th.join()
+        late[i] = (now - arrive[i]) * 1e3
+        owner[srv.submit(gids[w], k, s, row)] = (i, row, pool)
+    while owner:
+        drain(True)
     total = time.perf_counter() - t0
+    torch.cuda.synchronize()
     st = srv.stats()
     srv.close()
-    return lat, total, st, {i: outs[i] for i in keep}
+    return lat, total, st
 
 
 def extras_serving(ctx, args, local, g22):
     """Serving on 4 resident R-MAT graphs (scales 16/18/20/22, edge factor 16, int32
-    weights [1,255]; seeds 16/18/2/1) under a 40 GB budget: a 2,000-query sample of the
-    70/25/5 BFS/SSSP/MIS stream, first all at once (saturation), then Poisson arrivals at
-    about 0.8x and 2x the plain path's saturated rate. The plain path runs the same
-    stream one query at a time, FIFO; a sample of server answers is checked against it."""
-    import torch
-
+    weights [1,255]; seeds 16/18/2/1) under a 40 GB budget: the 100,000-query 70/25/5
+    BFS/SSSP/MIS stream (mt19937 seed 7), first all at once (saturation), then with Poisson
+    arrivals at 0.8x and 2x the plain path's saturated rate; and a BFS-only stream on the
+    scale-22 graph. The plain path runs each stream one query at a time, FIFO. Every answer
+    of every server run is compared with the plain path's answer to the same query (a
+    64-bit hash of each row, computed on the device)."""
     import apspie_b200 as ap
+    import torch
 
     dev = f"cuda:{local}"
     graphs = [ap.gen_rmat(16, 16, 16, 3), ap.gen_rmat(18, 16, 18, 3), ap.gen_rmat(20, 16, 2, 3), g22]
     dgs = [ap.DeviceGraph(g, dev) for g in graphs]
     prios = [torch.from_numpy(ap.mt19937_u32(4, g.m).view(np.int32)).to(dev) for g in graphs]
     n = SERVE_QUERIES
+    m_max = max(g.m for g in graphs)
     sat = serve_stream(graphs, n, 0.0)
     serve_plain(ctx, dgs, prios, serve_stream(graphs, 50, 0.0), dev)  # warm-up
-    lat_p, tot_p = serve_plain(ctx, dgs, prios, sat, dev)
+    ref = RowHasher(m_max, n, dev)
+    lat_p, tot_p = serve_plain(ctx, dgs, prios, sat, dev, ref)
+    ref_h = ref.result()
     plain_qps = n / tot_p
-    check = list(range(0, n, n // 40))
-    lat_s, tot_s, st, kept = serve_server(graphs, sat, dev, check)
-    exact = True
-    for i in check:
-        k, w, s = sat[0][i], sat[1][i], sat[2][i]
-        if k == 0:
-            ref = ctx.bfs(dgs[w], s)
-        elif k == 1:
-            ref = ctx.sssp(dgs[w], s)
-        else:
-            ref = ctx.mis(dgs[w], prios[w])
-        exact &= bool(torch.equal(ref, kept[i]))
+
+    def run_server(stream):
+        h = RowHasher(m_max, n, dev)
+        h.coef = ref.coef
+        lat_s, tot_s, st = serve_server(graphs, stream, dev, h)
+        return lat_s, tot_s, st, int((h.result() == ref_h).sum())
+
+    lat_s, tot_s, st, same = run_server(sat)
     res = {"serving": {
-        "workload": "4 graphs R-MAT s16/s18/s20/s22, 70/25/5 BFS/SSSP/MIS, 40 GB budget",
-        "slots": SERVE_SLOTS,
+        "workload": "4 graphs R-MAT s16/s18/s20/s22, 70/25/5 BFS/SSSP/MIS, 40 GB budget, 100,000 queries",
+        "slots": SERVE_SLOTS, "max_batch": SERVE_MAX_BATCH,
         "queries": n, "plain_qps": plain_qps, "server_qps": n / tot_s, "x_plain": tot_p / tot_s,
         "saturated": {"server": _pct(lat_s), "plain": _pct(lat_p)},
-        "launches": st["launches"], "max_batch_seen": st["max_batch_seen"], "peak_bytes": st["peak_bytes"],
-        "exact_checked": len(check), "exact": exact}}
-    # BFS-only stream on the scale-22 graph: the batched-serving target
-    words = ap.mt19937_u32(8, n).astype(np.int64)
-    bstream = (np.zeros(n, dtype=int), np.full(n, 3), [int(w % graphs[3].m) for w in words], np.zeros(n))
-    lat_p, tot_p = serve_plain(ctx, dgs, prios, bstream, dev)
-    lat_s, tot_s, st, _ = serve_server(graphs, bstream, dev)
-    res["serving"]["bfs_only_rmat22_saturated"] = {
-        "plain_qps": n / tot_p, "server_qps": n / tot_s, "x_plain": tot_p / tot_s, "server": _pct(lat_s),
-        "plain": _pct(lat_p), "launches": st["launches"], "max_batch_seen": st["max_batch_seen"]}
+        "launches": st["launches"], "joined_running": st["joined_running"], "trivial": st["trivial"],
+        "max_batch_seen": st["max_batch_seen"], "peak_bytes": st["peak_bytes"],
+        "exact_checked": n, "exact_equal": same, "exact": same == n}}
     for mult in (0.8, 2.0):
         rate = mult * plain_qps
         stream = serve_stream(graphs, n, rate)
-        lat_s, tot_s, _, _ = serve_server(graphs, stream, dev)
+        lat_s, tot_s, st, same = run_server(stream)
         lat_p, tot_p = serve_plain(ctx, dgs, prios, stream, dev)
         res["serving"][f"poisson_{mult}x_plain_rate"] = {
             "rate_qps": rate, "server": dict(_pct(lat_s), qps=n / tot_s),
-            "plain": dict(_pct(lat_p), qps=n / tot_p)}
+            "plain": dict(_pct(lat_p), qps=n / tot_p), "joined_running": st["joined_running"],
+            "exact_checked": n, "exact": same == n}
+    # BFS-only stream on the scale-22 graph: the batched-serving target
+    words = ap.mt19937_u32(8, n).astype(np.int64)
+    bstream = (np.zeros(n, dtype=int), np.full(n, 3), words % graphs[3].m, np.zeros(n))
+    bref = RowHasher(m_max, n, dev)
+    bref.coef = ref.coef
+    lat_p, tot_p = serve_plain(ctx, dgs, prios, bstream, dev, bref)
+    bref_h = bref.result()
+    h = RowHasher(m_max, n, dev)
+    h.coef = ref.coef
+    lat_s, tot_s, st = serve_server(graphs, bstream, dev, h)
+    same = int((h.result() == bref_h).sum())
+    res["serving"]["bfs_only_rmat22_saturated"] = {
+        "queries": n, "plain_qps": n / tot_p, "server_qps": n / tot_s, "x_plain": tot_p / tot_s,
+        "server": _pct(lat_s), "plain": _pct(lat_p), "launches": st["launches"],
+        "joined_running": st["joined_running"], "trivial": st["trivial"], "max_batch_seen": st["max_batch_seen"],
+        "exact_checked": n, "exact": same == n}
     return res
 
 
@@ -748,7 +846,7 @@ def main():
     ap_.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap_.add_argument("--no-extra", action="store_true")
     ap_.add_argument("--no-cpu-baseline", action="store_true")
-    ap_.add_argument("--only-extra", choices=["spgemm_tc", "build", "batched", "serving"], default=None,
+    ap_.add_argument("--only-extra", choices=["traversal", "spgemm_tc", "build", "batched", "serving"], default=None,
                      help="run one extra leg alone and print its JSON (no headline line)")
     args = ap_.parse_args()
     ws, rank, local = dist_env()
