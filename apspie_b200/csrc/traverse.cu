@@ -46,13 +46,22 @@ using BfsSmem = ExpandSmem<kBlock, kVT, false>;
 using BfsSlice = BfsSmem::Warp;
 constexpr int kSsspVT = APSPIE_SSSP_VT;
 constexpr int kSsspPA = 4;  // frontier entries per thread per phase-A step
+#ifndef APSPIE_SSSP_PIPE
+#define APSPIE_SSSP_PIPE 0  // 1: the expansion stages the next tile's entries with cp.async
+#endif
+#if APSPIE_SSSP_PIPE
+using SsspSmem = PipeSmem<kBlock, kSsspVT>;
+#else
 using SsspSmem = ExpandSmem<kBlock, kSsspVT, false>;
+#endif
 using SsspSlice = SsspSmem::Warp;
 using WQ = WarpQueue<Smem::QCAP>;
 
 struct NoPost {
     template <class S>
     __device__ void operator()(int, S &) const {}
+    template <class S>
+    __device__ void operator()(int, int, S &) const {}
 };
 
 constexpr int kInf = 0x7fffffff;
@@ -579,11 +588,8 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
         const int is_float = a.is_float;
         WQ wn(sm.qbuf[threadIdx.x >> 5][0], qn, qlen_next);
         WQ wf(sm.qbuf[threadIdx.x >> 5][1], fcur, flen);
-        frontier_expand<kBlock, kSsspVT, false>(
-            nf, E, a.buf.loc_off, a.buf.rs, sm,
-            [&](int j, int k, SsspSlice &ws) { ws.aux[k] = __ldcg(snap + j); },
-            [&](const bool (&valid)[kSsspVT], const int (&kk)[kSsspVT], const int (&idx)[kSsspVT],
-                SsspSlice &ws) {
+        auto relax = [&](const bool (&valid)[kSsspVT], const int (&kk)[kSsspVT], const int (&idx)[kSsspVT],
+                         auto &ws) {
                 constexpr int kVT = kSsspVT;
                 int v[kVT], we[kVT], cd[kVT], nd[kVT];
                 bool imp[kVT];
@@ -671,8 +677,15 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
                     wn.push(near[r], v[r]);
                     wf.push(far[r], v[r]);
                 }
-            },
-            NoPost(), vg, APSPIE_SSSP_CLAIM ? &a.ctl->claim : nullptr);
+            };
+#if APSPIE_SSSP_PIPE
+        frontier_expand_pipe<kBlock, kSsspVT>(nf, E, a.buf.loc_off, a.buf.rs, snap, sm, relax, NoPost(), vg,
+                                              APSPIE_SSSP_CLAIM ? &a.ctl->claim : nullptr);
+#else
+        frontier_expand<kBlock, kSsspVT, false>(
+            nf, E, a.buf.loc_off, a.buf.rs, sm, [&](int jj, int k, SsspSlice &w) { w.aux[k] = __ldcg(snap + jj); },
+            relax, NoPost(), vg, APSPIE_SSSP_CLAIM ? &a.ctl->claim : nullptr);
+#endif
         wn.flush();
         wf.flush();
         if (banded) {
