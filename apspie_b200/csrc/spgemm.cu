@@ -149,6 +149,9 @@ __global__ void sg_binlists(int m, const unsigned char *__restrict__ row_bin, in
     }
 }
 
+__device__ __forceinline__ void st_stream(float *p, float v) { __stcs(p, v); }
+__device__ __forceinline__ void st_stream(int *p, int v) { __stcs(p, v); }
+
 // ---------------------------------------------------------------- register (warp) tier
 template <int PL, typename V>
 struct RegTierSmem {
@@ -321,8 +324,10 @@ __global__ void __launch_bounds__(kSgBlock) sg_reg(const int *__restrict__ rows,
                     if ((kf >> QB) != col) break;
                     sum = vadd<V>(sum, sm.pv[kf & QMASK]);
                 }
-                cci[c0 + rank] = static_cast<int>(col);
-                cval[c0 + rank] = sum;
+                // streaming stores: C is written once and never re-read here, so it should
+                // not push B (re-read by every row that names it) out of L2
+                __stcs(cci + c0 + rank, static_cast<int>(col));
+                st_stream(cval + c0 + rank, sum);
             }
             before += __popc(hmask[r]);
         }
@@ -504,8 +509,8 @@ __global__ void __launch_bounds__(kSgBlock) sg_block(const int *__restrict__ row
                     const int off = static_cast<int>(k - w0);
                     const int word = off >> 5;
                     const int rank = sm.wpre[word] + __popc(sm.bits[word] & ((1u << (off & 31)) - 1u));
-                    cci[c0 + done + rank] = k;
-                    cval[c0 + done + rank] = GLOBAL ? __ldcg(vals + s) : vals[s];
+                    __stcs(cci + c0 + done + rank, k);
+                    st_stream(cval + c0 + done + rank, GLOBAL ? __ldcg(vals + s) : vals[s]);
                 }
             }
             done += tot;
