@@ -239,11 +239,13 @@ __device__ __forceinline__ int *depth_row(const MsArgs &a, int q) {
 }
 
 // Writes depth L + 1 of vertex v for query slot q (in the engine: relative to the level the
-// query started at, and to the row its request gave).
+// query started at, and into the row its request gave; both are copied into shared memory
+// at the start of every level: s_row, s_base).
 template <bool SERVE>
-__device__ __forceinline__ void put_depth(const MsArgs &a, int q, int v, int L) {
+__device__ __forceinline__ void put_depth(const MsArgs &a, int q, int v, int L, int *const *s_row,
+                                          const int *s_base) {
     if (SERVE)
-        reinterpret_cast<int *const volatile *>(a.sv->rows)[q][v] = L + 1 - __ldcg(&a.sv->start[q]);
+        s_row[q][v] = L + 1 - s_base[q];
     else
         depth_row(a, q)[v] = L + 1;
 }
@@ -265,6 +267,8 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
     __shared__ MsSmem sm;
     __shared__ unsigned s_qmask[W];   // query slots in flight this level
     __shared__ unsigned s_alive[W];   // bits this block found in the next frontier (engine)
+    __shared__ int *s_row[SERVE ? 32 * W : 1];  // engine: each slot's output row this level
+    __shared__ int s_base[SERVE ? 32 * W : 1];  // engine: each slot's start level
     timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
     const int gtid = blockIdx.x * kMsBlock + threadIdx.x;
@@ -347,6 +351,10 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
             if (!grid_barrier(a.ctl, a.sticky, kSiteMs + 6)) return;
             if (ld_volatile_i32(&a.sv->exit_flag)) break;
             if (threadIdx.x < W) s_qmask[threadIdx.x] = __ldcg(&a.sv->active[threadIdx.x]);
+            for (int q = threadIdx.x; q < 32 * W; q += blockDim.x) {
+                s_row[SERVE ? q : 0] = reinterpret_cast<int *const volatile *>(a.sv->rows)[q];
+                s_base[SERVE ? q : 0] = __ldcg(&a.sv->start[q]);
+            }
             // first phase of the level: the admitted queries' output rows (0 at the source,
             // -1 elsewhere), and the sweep of retired slots' visited bits
             const int nadm = ld_volatile_i32(&a.sv->adm_n);
@@ -460,7 +468,7 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
                             while (b) {
                                 const int bit = __ffs(b) - 1;
                                 b &= b - 1;
-                                put_depth<SERVE>(a, w * 32 + bit, v, L);
+                                put_depth<SERVE>(a, w * 32 + bit, v, L, s_row, s_base);
                             }
                         }
                     }
@@ -536,7 +544,7 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
                     while (anyb) {
                         const int bit = __ffs(anyb) - 1;
                         anyb &= anyb - 1;
-                        if ((got[w] >> bit) & 1u) put_depth<SERVE>(a, w * 32 + bit, v, L);
+                        if ((got[w] >> bit) & 1u) put_depth<SERVE>(a, w * 32 + bit, v, L, s_row, s_base);
                     }
                     if (SERVE) {
                         const unsigned wa = __reduce_or_sync(lanemask_all, got[w]);
@@ -599,7 +607,7 @@ __global__ void __launch_bounds__(kMsBlock, W >= 16 ? 3 : 4) msbfs_kernel(MsArgs
                             while (b) {
                                 const int bit = __ffs(b) - 1;
                                 b &= b - 1;
-                                put_depth<SERVE>(a, threadIdx.x * 32 + bit, v, L);
+                                put_depth<SERVE>(a, threadIdx.x * 32 + bit, v, L, s_row, s_base);
                             }
                         }
                     }
