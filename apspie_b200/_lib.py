@@ -133,6 +133,7 @@ SIGNATURES = {
     "apspie_sssp_f32": (c_int, [c_void_p, POINTER(CSR), c_int32, c_void_p, c_float, POINTER(RunStats)]),
     "apspie_mis_int32": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p, POINTER(RunStats)]),
     "apspie_spmspv_bool": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p]),
+    "apspie_row_checksums": (c_int, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
     "apspie_spmspv": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_void_p, c_int32, c_void_p, c_void_p,
                               POINTER(c_int32)]),
     "apspie_bfs_batch": (c_int, [c_void_p, POINTER(CSR), c_void_p, c_int32, c_int32, c_void_p,

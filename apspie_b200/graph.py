@@ -371,6 +371,18 @@ class Context:
                                           ctypes.byref(ny)), "spmspv")
         return y_ind[: ny.value], y_val[: ny.value]
 
+    def row_checksums(self, rows, slots, coef, out) -> None:
+        """out[slots[k]] += sum_i rows[k][i] * coef[i] (int32 products, int64 sum) for CUDA
+        tensors rows[k] (int32 or uint8, equal length), coef (int32), out (int64, zeroed)."""
+        n = len(rows)
+        if n == 0:
+            return
+        ptrs = (ctypes.c_void_p * n)(*[r.data_ptr() for r in rows])
+        sl = np.ascontiguousarray(slots, dtype=np.int32)
+        eb = 1 if rows[0].element_size() == 1 else 4
+        self._check(L.lib().apspie_row_checksums(self.handle, ptrs, sl.ctypes.data, n, int(rows[0].shape[0]), eb,
+                                                 coef.data_ptr(), out.data_ptr()), "row_checksums")
+
     # ---- batched traversal
     def bfs_batch_into(self, g: DeviceGraph, sources, out, depth_cap: int = 0, stats: bool = False):
         """sources: int32 CUDA tensor [nq]; out: int32 CUDA tensor [nq, m] (query-major)."""

@@ -555,10 +555,10 @@ def extras_batched(ctx, args, ws, local, g):
     res = {"plain_bfs_rmat22": {"ms_per_query": plain_ms, "queries_per_s": ws * 1e3 / plain_ms}}
     # every batched row is compared with the plain path's answer for its source (row hashes),
     # and row 0 with the oracle
-    ref = RowHasher(g.m, 512, dev)
+    ref = RowHasher(ctx, g.m, 512, dev)
     for q, x in enumerate(srcs):
         ctx.bfs_into(dg, int(x), one)
-        ref.put(q, one)
+        ref.put_now(q, one)
     ref_h = ref.result()
     for nq in (32, 128, 512):
         s = torch.from_numpy(srcs[:nq]).to(dev)
@@ -566,8 +566,7 @@ def extras_batched(ctx, args, ws, local, g):
         ctx.bfs_batch_into(dg, s, out)
         tot, per = time_steps(ctx.stream, lambda: ctx.bfs_batch_into(dg, s, out), 3)
         ms = max_over_ranks(ws, tot / 3)
-        h = RowHasher(g.m, nq, dev)
-        h.coef = ref.coef
+        h = RowHasher(ctx, g.m, nq, dev, ref.coef)
         for q in range(nq):
             h.put(q, out[q])
         same = int((h.result() == ref_h[:nq]).sum())
@@ -582,10 +581,10 @@ def extras_batched(ctx, args, ws, local, g):
     tot, _ = time_steps(ctx.stream, lambda: [ctx.sssp_into(dg, int(x), one) for x in srcs[:16]], 1)
     plain_ms = max_over_ranks(ws, tot / 16)
     res["plain_sssp_rmat22"] = {"ms_per_query": plain_ms, "queries_per_s": ws * 1e3 / plain_ms}
-    ref = RowHasher(g.m, 512, dev)
+    ref = RowHasher(ctx, g.m, 512, dev)
     for q, x in enumerate(srcs):
         ctx.sssp_into(dg, int(x), one)
-        ref.put(q, one)
+        ref.put_now(q, one)
     ref_h = ref.result()
     for nq in (32, 128, 512):
         s = torch.from_numpy(srcs[:nq]).to(dev)
@@ -594,8 +593,7 @@ def extras_batched(ctx, args, ws, local, g):
         reps = 3 if nq < 512 else 1
         tot, per = time_steps(ctx.stream, lambda: ctx.sssp_batch_into(dg, s, out), reps)
         ms = max_over_ranks(ws, tot / reps)
-        h = RowHasher(g.m, nq, dev)
-        h.coef = ref.coef
+        h = RowHasher(ctx, g.m, nq, dev, ref.coef)
         for q in range(nq):
             h.put(q, out[q])
         same = int((h.result() == ref_h[:nq]).sum())
@@ -615,26 +613,47 @@ POOL_ROWS = 512  # output rows per graph a stream keeps in flight (int32 rows; M
 
 
 class RowHasher:
-    """A 64-bit linear hash of a result row, computed on the device without a host sync:
-    h = sum_i row[i] * c[i] (int32 products, int64 sum; exact, so order-independent) with
-    per-position coefficients drawn once. Equal rows give equal hashes; a differing row
-    collides only with probability about 2^-32."""
+    """A 64-bit linear checksum of each result row, computed on the device by the library
+    (apspie_row_checksums) without a host sync: h = sum_i row[i] * c[i] (int32 products,
+    int64 sum; exact, so order-independent) with per-position coefficients drawn once.
+    Equal rows give equal checksums; a differing row collides only with probability about
+    2^-32. Rows are checksummed in groups of up to 128 per launch, on the given context's
+    stream; put_now() checksums a row at once (for a buffer that is about to be reused)."""
 
-    def __init__(self, m_max, n, dev):
+    def __init__(self, ctx, m_max, n, dev, coef=None):
         import torch
 
-        g = torch.Generator(device="cpu").manual_seed(12345)
-        self.coef = torch.randint(-(1 << 31), (1 << 31) - 1, (m_max,), generator=g, dtype=torch.int64)
-        self.coef = self.coef.to(torch.int32).to(dev)
+        self.ctx = ctx
+        if coef is None:
+            g = torch.Generator(device="cpu").manual_seed(12345)
+            coef = torch.randint(-(1 << 31), (1 << 31) - 1, (m_max,), generator=g, dtype=torch.int64)
+            coef = coef.to(torch.int32).to(dev)
+        self.coef = coef
         self.out = torch.zeros(n, dtype=torch.int64, device=dev)
+        self.rows, self.slots = [], []
 
     def put(self, i, row):
-        import torch
+        self.rows.append(row)
+        self.slots.append(i)
+        if len(self.rows) >= 128:
+            self.flush()
 
-        c = self.coef[: row.shape[0]]
-        self.out[i] = torch.sum(row.to(torch.int32) * c, dtype=torch.int64)
+    def put_now(self, i, row):
+        self.put(i, row)
+        self.flush()
+
+    def flush(self):
+        groups = {}
+        for r, i in zip(self.rows, self.slots):
+            groups.setdefault((r.shape[0], r.element_size()), ([], []))
+            groups[(r.shape[0], r.element_size())][0].append(r)
+            groups[(r.shape[0], r.element_size())][1].append(i)
+        for rows, slots in groups.values():
+            self.ctx.row_checksums(rows, slots, self.coef, self.out)
+        self.rows, self.slots = [], []
 
     def result(self):
+        self.flush()
         return self.out.cpu().numpy()
 
 
@@ -687,9 +706,8 @@ def serve_plain(ctx, dgs, prios, stream, dev, hasher=None):
             ctx.mis_into(dgs[w], prios[w], mis_out[w])
         ctx.synchronize()
         lat[i] = (time.perf_counter() - t0 - arrive[i]) * 1e3
-        if hasher is not None:
-            with torch.cuda.stream(ctx.stream):
-                hasher.put(i, mis_out[w] if k == 2 else outs[w])
+        if hasher is not None:  # on the library's stream, before the buffer is reused
+            hasher.put_now(i, mis_out[w] if k == 2 else outs[w])
     total = time.perf_counter() - t0
     torch.cuda.synchronize()
     return lat, total
@@ -743,6 +761,7 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None):
             hasher.put(i, row)
             hashed.append((row, pool))
         if hashed and (block or len(hashed) >= 256):
+            hasher.flush()
             torch.cuda.current_stream().synchronize()
             for row, pool in hashed:
                 pool.append(row)
@@ -790,14 +809,14 @@ def extras_serving(ctx, args, local, g22):
     m_max = max(g.m for g in graphs)
     sat = serve_stream(graphs, n, 0.0)
     serve_plain(ctx, dgs, prios, serve_stream(graphs, 50, 0.0), dev)  # warm-up
-    ref = RowHasher(m_max, n, dev)
+    ref = RowHasher(ctx, m_max, n, dev)
     lat_p, tot_p = serve_plain(ctx, dgs, prios, sat, dev, ref)
     ref_h = ref.result()
     plain_qps = n / tot_p
+    hctx = ap.Context(local)  # the server leg's checksums run on torch's current stream
 
     def run_server(stream):
-        h = RowHasher(m_max, n, dev)
-        h.coef = ref.coef
+        h = RowHasher(hctx, m_max, n, dev, ref.coef)
         lat_s, tot_s, st = serve_server(graphs, stream, dev, h)
         return lat_s, tot_s, st, int((h.result() == ref_h).sum())
 
@@ -822,14 +841,13 @@ def extras_serving(ctx, args, local, g22):
     # BFS-only stream on the scale-22 graph: the batched-serving target
     words = ap.mt19937_u32(8, n).astype(np.int64)
     bstream = (np.zeros(n, dtype=int), np.full(n, 3), words % graphs[3].m, np.zeros(n))
-    bref = RowHasher(m_max, n, dev)
-    bref.coef = ref.coef
+    bref = RowHasher(ctx, m_max, n, dev, ref.coef)
     lat_p, tot_p = serve_plain(ctx, dgs, prios, bstream, dev, bref)
     bref_h = bref.result()
-    h = RowHasher(m_max, n, dev)
-    h.coef = ref.coef
+    h = RowHasher(hctx, m_max, n, dev, ref.coef)
     lat_s, tot_s, st = serve_server(graphs, bstream, dev, h)
     same = int((h.result() == bref_h).sum())
+    hctx.close()
     res["serving"]["bfs_only_rmat22_saturated"] = {
         "queries": n, "plain_qps": n / tot_p, "server_qps": n / tot_s, "x_plain": tot_p / tot_s,
         "server": _pct(lat_s), "plain": _pct(lat_p), "launches": st["launches"],

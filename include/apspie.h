@@ -300,6 +300,17 @@ apspie_status apspie_spmspv_bool(apspie_ctx *ctx, const apspie_csr *A, const int
 apspie_status apspie_spmspv(apspie_ctx *ctx, const apspie_csr *A, const int32_t *d_x_ind, const void *d_x_val,
                             int32_t x_nnz, int32_t *d_y_ind, void *d_y_val, int32_t *y_nnz);
 
+/* Checksums of result rows, to check many answers against a reference without copying
+ * them to the host: for each k < nrows, d_out[h_slots[k]] += sum_i row_k[i] * d_coef[i]
+ * over i < m, with row_k = h_rows[k] (device memory; int32 elements for elem_bytes 4,
+ * uint8 for 1), int32 products (wrapping) and an exact int64 sum, so the value does not
+ * depend on the order of the additions. h_rows / h_slots are host arrays; zero the d_out
+ * slots first. Asynchronous on the context's stream. No reference counterpart (the
+ * reference compares whole result vectors on the host, src/util.cuh:260-269). */
+apspie_status apspie_row_checksums(apspie_ctx *ctx, const void *const *h_rows, const int32_t *h_slots,
+                                   int32_t nrows, int32_t m, int32_t elem_bytes, const int32_t *d_coef,
+                                   int64_t *d_out);
+
 /* ---- SpGEMM and triangle counting ---------------------------------------------- */
 
 /* C = A * B, row-binned hash Gustavson. A and B share val_type (F32 or I32). C's rows are

@@ -69,3 +69,23 @@ def test_spmspv_rejects_index_out_of_range_and_context_survives(ctx):
     oi, ov = oracle.spmspv(g.row_ptr, g.col_ind, val, g.n, x, xv)
     np.testing.assert_array_equal(yi.cpu().numpy(), oi)
     np.testing.assert_array_equal(yv.cpu().numpy(), ov)
+
+
+def test_row_checksums_match_a_torch_computation(ctx):
+    """apspie_row_checksums equals sum(row * coef) computed by torch (int32 products,
+    int64 sum), for int32 and uint8 rows, several rows per launch and more than one launch."""
+    import torch
+
+    m = 100_003
+    g = torch.Generator().manual_seed(3)
+    coef = torch.randint(-(1 << 31), (1 << 31) - 1, (m,), generator=g, dtype=torch.int64).to(torch.int32).cuda()
+    rows = [torch.randint(-1, 40, (m,), generator=g, dtype=torch.int32).cuda() for _ in range(300)]
+    out = torch.zeros(310, dtype=torch.int64, device="cuda")
+    slots = list(range(5, 305))
+    ctx.row_checksums(rows, slots, coef, out)
+    ref = torch.stack([torch.sum(r * coef, dtype=torch.int64) for r in rows])
+    assert torch.equal(out[5:305], ref) and int(out[:5].abs().sum()) == 0
+    u8 = [torch.randint(0, 2, (m,), generator=g, dtype=torch.uint8).cuda() for _ in range(3)]
+    o8 = torch.zeros(3, dtype=torch.int64, device="cuda")
+    ctx.row_checksums(u8, [0, 1, 2], coef, o8)
+    assert torch.equal(o8, torch.stack([torch.sum(r.to(torch.int32) * coef, dtype=torch.int64) for r in u8]))
