@@ -810,8 +810,10 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_group_kernel(Ss
 // ================================================================================
 // MIS
 // ================================================================================
-enum : unsigned char { kUndecided = 0, kIn = 1, kOut = 2, kScan = 3 };
+enum : unsigned char { kUndecided = 0, kIn = 1, kOut = 2 };
 constexpr int kJoinEntry = static_cast<int>(0x80000000u);  // queue entry: a vertex that joined
+constexpr int kMisGroup = 8;   // lanes that scan one vertex's row together
+constexpr int kMisChunks = 4;  // chunks of kMisGroup neighbours a group scans before handing on
 
 struct MisArgs {
     int m, nnz;
@@ -822,10 +824,14 @@ struct MisArgs {
     int *member_i32;  // when set, the set is written here as int32 1/0 instead
     unsigned char *state;
     int *pos;    // CSR index of the outranking neighbour that blocks the vertex (row start - 1: none yet)
-    int *first;  // least CSR index of a stop found by this round's scan (kInf: none)
+    int *longq;  // vertices whose scan continues past kMisGroup * kMisChunks neighbours this round
     TravBuffers buf;
     TravCtl *ctl;
     int *sticky;
+};
+
+struct RowOfMisEntry {
+    __device__ __forceinline__ int operator()(int e) const { return e & ~kJoinEntry; }
 };
 
 __device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v) {
@@ -842,47 +848,62 @@ __device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v)
 // join while the vertex is undecided), and a neighbour once seen out or lower-ranked
 // stays so. So each undecided vertex keeps a scan position `pos`: every neighbour before
 // it is settled, and the neighbour at it is its current blocker (undecided, outranking).
-// Its row is read once over the whole run instead of once per round. Round r, over a
-// queue holding the undecided vertices and the vertices that joined in round r-1:
-//  phase A  a joined vertex enters with its whole row (to knock its neighbours out);
-//           an undecided vertex re-checks its blocker: still undecided -> nothing to do
-//           this round; out (or no blocker yet) -> it enters with the rest of its row
-//           after pos (state kScan); in -> its push this round knocks the vertex out;
-//  phase B  merge-path expansion of those segments: a joined vertex's edges write out
-//           into its neighbours; a scanning vertex's edges look for the first neighbour
-//           that outranks it and is not out (the least CSR index per vertex: shared
-//           atomicMin per tile, then one global atomicMin per vertex and tile);
-//  phase C  a scanned vertex with no stop joins (and is queued to push next round); one
-//           with a stop keeps it as its new blocker; out vertices leave the queue.
-// Reads of the state during phase B race with its out-writes only in the safe direction
-// (an undecided neighbour that is being knocked out only stops a scan early, and the
-// blocker check of the next round resumes it), so the set is the greedy MIS whatever the
-// timing; R-MAT scale 20 settles in 6 rounds with about 1.1 edge reads per edge.
+// A row is read about once over the whole run, and each scan stops at the first
+// neighbour that decides anything: about 1.5M neighbour reads for R-MAT scale 20's 31.4M
+// entries. Vertices without neighbours join at the start. Round r, over a queue holding
+// the undecided vertices and the vertices that joined in round r-1:
+//  phase A  row lengths of the joined vertices (merge-path scan);
+//  phase P  the joined vertices write out into their neighbours (merge-path expansion);
+//  phase S  each undecided vertex, by a group of kMisGroup lanes: out -> leaves; its
+//           blocker still undecided (or in: its push comes next round) -> waits; else it
+//           scans the rest of its row in chunks of kMisGroup, stopping at the first
+//           neighbour that outranks it and is not out (its new blocker); no such neighbour
+//           -> it joins (and is queued to push next round). After kMisChunks chunks without
+//           an end the vertex goes to the long list;
+//  phase L  (only when the long list is not empty) one block per listed vertex scans on to
+//           its stop or its row's end.
+// The pushes of a round are complete before its scans start, so a scan sees every
+// vertex knocked out so far; scans and joins of the same phase race only safely (a vertex
+// joins only if every outranking neighbour was seen out, and out is final). The set is
+// the greedy MIS whatever the timing.
 __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
     __shared__ Smem sm;
+    __shared__ int s_stop;
     timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
     const int gtid = blockIdx.x * kBlock + threadIdx.x;
     const int gstride = G * kBlock;
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
     const int m = a.m;
-    for (int i = gtid; i < m; i += gstride) {
-        a.state[i] = kUndecided;
-        a.pos[i] = __ldg(a.row_ptr + i) - 1;
-        a.first[i] = kInf;
-        a.buf.q0[i] = i;
-    }
-    if (gtid == 0) {
-        a.ctl->qlen[0] = m;
-        a.ctl->qlen[1] = 0;
-    }
-    if (!grid_barrier(a.ctl, a.sticky, kSiteMis)) return;
-
-    int cur = 0;
-    long long expanded = 0;
-    int round = 0;
     const int *col = a.col_ind;
     const unsigned *prio = a.prio;
     unsigned char *state = a.state;
+    int *l2len = &a.ctl->flen[0];
+    {
+        WQ wq(sm.qbuf[wid][0], a.buf.q0, &a.ctl->qlen[0]);
+        for (int base = blockIdx.x * kBlock; base < m; base += gstride) {
+            const int v = base + threadIdx.x;
+            bool q = false;
+            if (v < m) {
+                const int r0 = __ldg(a.row_ptr + v);
+                q = __ldg(a.row_ptr + v + 1) > r0;
+                a.state[v] = q ? kUndecided : kIn;  // no neighbours: in the set from the start
+                a.pos[v] = r0 - 1;
+            }
+            wq.push(q, v);
+        }
+        wq.flush();
+    }
+    if (gtid == 0) a.ctl->qlen[1] = 0;
+    if (!grid_barrier(a.ctl, a.sticky, kSiteMis)) return;
+
+    int cur = 0;
+    long long expanded = 0, scanned = 0;
+    int round = 0;
+    const int g8 = lane / kMisGroup, l8 = lane % kMisGroup;
+    const unsigned gmask = ((1u << kMisGroup) - 1u) << (g8 * kMisGroup);
+    constexpr int kGroupsPerWarp = 32 / kMisGroup;
     for (;;) {
         const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
         if (nf == 0) break;
@@ -895,124 +916,136 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         int *qn = cur ? a.buf.q0 : a.buf.q1;
         int *qlen_next = &a.ctl->qlen[cur ^ 1];
 
-        // phase A: segment of every entry (row start in rs, length scanned into loc_off)
-        {
-            const int C = (nf + G - 1) / G;
-            const int c0 = min(blockIdx.x * C, nf);
-            const int c1 = min(c0 + C, nf);
-            int carry = 0;
-            for (int base = c0; base < c1; base += kBlock) {
-                const int i = base + threadIdx.x;
-                int len = 0;
-                if (i < c1) {
-                    const int e = __ldcg(qc + i);
-                    const int v = e & ~kJoinEntry;
-                    const int r0 = __ldg(a.row_ptr + v), r1 = __ldg(a.row_ptr + v + 1);
-                    int start = r0;
-                    if (e & kJoinEntry) {
-                        len = r1 - r0;
-                    } else {
-                        const int p = __ldcg(a.pos + v);
-                        bool scan = true;
-                        if (p >= r0) scan = __ldcg(state + __ldg(col + p)) == kOut;
-                        if (scan) {
-                            state[v] = kScan;
-                            start = p + 1;
-                            len = r1 - start;
-                        }
-                    }
-                    a.buf.rs[i] = start;
-                }
-                int tot;
-                const int ex = block_exclusive_scan<kBlock>(len, tot, sm.scan_tmp);
-                if (i < c1) a.buf.loc_off[i] = carry + ex;
-                carry += tot;
-            }
-            if (threadIdx.x == 0) a.buf.chunk_sum[blockIdx.x] = carry;
-        }
+        // phase A: row lengths of the joined vertices (undecided entries expand nothing)
+        frontier_phase_a<kBlock>(qc, nf, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum, sm.scan_tmp,
+                                 [](int, int e, int deg) { return (e & kJoinEntry) ? deg : 0; }, RowOfMisEntry{});
         if (gtid == 0) {
             *qlen_next = 0;
-            a.ctl->claim = 0;
+            *l2len = 0;
         }
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 1)) return;
 
-        // phase B: pushes and scans
+        // phase P: knock-outs
         const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
-        expanded += E;
-        int *first = a.first;
-        frontier_expand<kBlock, kVT, true, false>(
-            nf, E, a.buf.loc_off, a.buf.rs, sm,
-            [&](int j, int k, WarpSlice &ws) {
-                const int e = __ldcg(qc + j);
-                ws.aux[k] = e;
-                ws.aux2[k] = (e & kJoinEntry) ? 0 : static_cast<int>(__ldg(prio + e));
-                ws.flag[k] = kInf;
-            },
-            [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT], WarpSlice &ws) {
-                int u[kVT];
-                unsigned pu[kVT];
-                unsigned char su[kVT];
+        if (E > 0) {
+            expanded += E;
+            frontier_expand<kBlock, kVT, true, false>(
+                nf, E, a.buf.loc_off, a.buf.rs, sm,
+                [&](int j, int k, WarpSlice &ws) { ws.aux[k] = __ldcg(qc + j) & ~kJoinEntry; },
+                [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT], WarpSlice &ws) {
+                    int u[kVT];
 #pragma unroll
-                for (int r = 0; r < kVT; ++r) u[r] = valid[r] ? __ldg(col + idx[r]) : 0;
+                    for (int r = 0; r < kVT; ++r) u[r] = valid[r] ? __ldg(col + idx[r]) : 0;
 #pragma unroll
-                for (int r = 0; r < kVT; ++r) {
-                    const bool scan = valid[r] && !(ws.aux[kk[r]] & kJoinEntry);
-                    pu[r] = scan ? __ldg(prio + u[r]) : 0u;
-                    su[r] = scan ? __ldcg(state + u[r]) : kOut;
-                }
-#pragma unroll
-                for (int r = 0; r < kVT; ++r) {
-                    if (!valid[r]) continue;
-                    const int e = ws.aux[kk[r]];
-                    const int v = e & ~kJoinEntry;
-                    if (u[r] == v) continue;  // self-loops decide nothing
-                    if (e & kJoinEntry)
-                        state[u[r]] = kOut;  // a neighbour of a set vertex (never in the set itself)
-                    else if (su[r] != kOut && outranks(pu[r], u[r], static_cast<unsigned>(ws.aux2[kk[r]]), v))
-                        atomicMin(&ws.flag[kk[r]], idx[r]);
-                }
-            },
-            [&](int ne, WarpSlice &ws) {
-                for (int k = threadIdx.x & 31; k < ne; k += 32) {
-                    const int f = ws.flag[k];
-                    if (f != kInf) atomicMin(first + ws.aux[k], f);
-                }
-            },
-            hw_grid(), APSPIE_TRAV_CLAIM ? &a.ctl->claim : nullptr);
-        if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 2)) return;
+                    for (int r = 0; r < kVT; ++r)
+                        if (valid[r] && u[r] != ws.aux[kk[r]]) state[u[r]] = kOut;  // never in the set
+                },
+                NoPost());
+            if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 2)) return;
+        }
 
-        // phase C: decisions
-        WQ wq(sm.qbuf[threadIdx.x >> 5][0], qn, qlen_next);
-        for (int base = blockIdx.x * kBlock; base < nf; base += gstride) {
-            const int i = base + threadIdx.x;
-            bool keep = false;
-            int out = 0;
-            if (i < nf) {
-                const int e = __ldcg(qc + i);
-                if (!(e & kJoinEntry)) {
-                    const unsigned char s = __ldcg(state + e);
-                    if (s == kUndecided) {
-                        keep = true;
-                        out = e;
-                    } else if (s == kScan) {
-                        const int f = __ldcg(first + e);
-                        keep = true;
-                        if (f == kInf) {
-                            state[e] = kIn;
-                            out = e | kJoinEntry;
-                        } else {
-                            a.pos[e] = f;
-                            first[e] = kInf;
-                            state[e] = kUndecided;
-                            out = e;
+        // phase S: blocker checks, scans, decisions (kGroupsPerWarp vertices per warp)
+        {
+            WQ wq(sm.qbuf[wid][0], qn, qlen_next);
+            WQ wl(sm.qbuf[wid][1], a.longq, l2len);
+            const int gw = gtid >> 5, nw = gstride >> 5;
+            for (int wb = gw * kGroupsPerWarp; wb < nf; wb += nw * kGroupsPerWarp) {
+                const int i = wb + g8;
+                const int e = i < nf ? __ldcg(qc + i) : kJoinEntry;
+                const int v = e & ~kJoinEntry;
+                bool scanning = false, keep = false, joined = false, handed = false;
+                int start = 0, r1 = 0;
+                unsigned pv = 0;
+                if (!(e & kJoinEntry) && __ldcg(state + v) == kUndecided) {
+                    const int r0 = __ldg(a.row_ptr + v);
+                    r1 = __ldg(a.row_ptr + v + 1);
+                    const int p = __ldcg(a.pos + v);
+                    scanning = p < r0 || __ldcg(state + __ldg(col + p)) == kOut;
+                    keep = !scanning;  // its blocker is undecided, or joined (and pushes next round)
+                    start = p + 1;
+                    pv = __ldg(prio + v);
+                }
+                int stop = -1;
+                bool done = !scanning;
+#pragma unroll
+                for (int c = 0; c < kMisChunks; ++c) {
+                    const int idx = start + c * kMisGroup + l8;
+                    bool st = false;
+                    if (!done && idx < r1) {
+                        const int u = __ldg(col + idx);
+                        const unsigned pu = __ldg(prio + u);
+                        const unsigned char su = __ldcg(state + u);
+                        st = u != v && su != kOut && outranks(pu, u, pv, v);
+                    }
+                    const unsigned b = __ballot_sync(0xffffffffu, st) & gmask;
+                    if (!done) {
+                        if (b) {
+                            stop = start + c * kMisGroup + (__ffs(b) - 1 - g8 * kMisGroup);
+                            done = true;
+                        } else if (start + (c + 1) * kMisGroup >= r1) {
+                            joined = true;
+                            done = true;
                         }
                     }
                 }
+                if (scanning) {
+                    if (l8 == 0) scanned += min(r1, stop >= 0 ? stop + 1 : start + kMisChunks * kMisGroup) - start;
+                    if (stop >= 0) {
+                        keep = true;
+                        if (l8 == 0) a.pos[v] = stop;
+                    } else if (joined) {
+                        keep = true;
+                        if (l8 == 0) state[v] = kIn;
+                    } else {
+                        handed = true;  // settled up to start + kMisChunks * kMisGroup - 1
+                        if (l8 == 0) a.pos[v] = start + kMisChunks * kMisGroup - 1;
+                    }
+                }
+                wq.push(keep && l8 == 0, joined ? (v | kJoinEntry) : v);
+                wl.push(handed && l8 == 0, v);
             }
-            wq.push(keep, out);
+            wq.flush();
+            wl.flush();
         }
-        wq.flush();
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 3)) return;
+
+        // phase L: the long scans, one block per vertex
+        const int nl = ld_volatile_i32(l2len);
+        if (nl > 0) {
+            for (int k = blockIdx.x; k < nl; k += G) {
+                const int v = __ldcg(a.longq + k);
+                const int r1 = __ldg(a.row_ptr + v + 1);
+                const int start = __ldcg(a.pos + v) + 1;
+                const unsigned pv = __ldg(prio + v);
+                if (threadIdx.x == 0) s_stop = kInf;
+                __syncthreads();
+                for (int b0 = start; b0 < r1; b0 += kBlock) {
+                    const int idx = b0 + threadIdx.x;
+                    bool st = false;
+                    if (idx < r1) {
+                        const int u = __ldg(col + idx);
+                        const unsigned pu = __ldg(prio + u);
+                        const unsigned char su = __ldcg(state + u);
+                        st = u != v && su != kOut && outranks(pu, u, pv, v);
+                    }
+                    if (st) atomicMin(&s_stop, idx);
+                    if (__syncthreads_or(st)) break;
+                }
+                if (threadIdx.x == 0) {
+                    const int sp = s_stop;
+                    scanned += (sp != kInf ? sp + 1 : r1) - start;
+                    if (sp != kInf) {
+                        a.pos[v] = sp;
+                        qn[atomicAdd(qlen_next, 1)] = v;
+                    } else {
+                        state[v] = kIn;
+                        qn[atomicAdd(qlen_next, 1)] = v | kJoinEntry;
+                    }
+                }
+                __syncthreads();
+            }
+            if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 4)) return;
+        }
         cur ^= 1;
     }
     long long insz = 0;
@@ -1024,14 +1057,21 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
             a.member[i] = (s == kIn) ? 1 : 0;
         insz += (s == kIn);
     }
-    for (int o = 16; o; o >>= 1) insz += __shfl_down_sync(0xffffffffu, insz, o);
+    for (int o = 16; o; o >>= 1) {
+        insz += __shfl_down_sync(0xffffffffu, insz, o);
+        scanned += __shfl_down_sync(0xffffffffu, scanned, o);
+    }
     if ((threadIdx.x & 31) == 0 && insz)
         atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->vertices_reached),
                   static_cast<unsigned long long>(insz));
+    if ((threadIdx.x & 31) == 0 && scanned)
+        atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->edges_expanded),
+                  static_cast<unsigned long long>(scanned));
     if (gtid == 0) {
         a.ctl->iterations = round;
         a.ctl->push_iterations = round;
-        a.ctl->edges_expanded = expanded;
+        atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->edges_expanded),
+                  static_cast<unsigned long long>(expanded));
         a.ctl->edges_component = a.nnz;
     }
 }
@@ -1389,7 +1429,7 @@ static apspie_status mis_common(apspie_ctx *ctx, const apspie_csr *A, const uint
     a.member_i32 = d_member_i32;
     a.buf = carve_trav(base, A->m);
     a.pos = a.buf.aux;
-    a.first = a.buf.aux2;
+    a.longq = a.buf.q2;
     Carver c(static_cast<char *>(base) + tb);
     a.state = c.take<unsigned char>(A->m);
     a.ctl = ctx->d_ctl;

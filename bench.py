@@ -376,10 +376,14 @@ def extras(ctx, args, ws, local):
     traversal and serving."""
     import apspie_b200 as ap
 
+    _progress("extra: traversal")
     res = extras_traversal(ctx, args, ws, local)
+    _progress("extra: spgemm / tc")
     res.update(extras_spgemm_tc(ctx, args, ws, local))
+    _progress("extra: device construction")
     res.update(extras_build(ctx, args, ws, local))
     g22 = ap.gen_rmat(22, 16, 1, 3)  # weights for the serving leg; BFS ignores them
+    _progress("extra: batched traversal")
     res.update(extras_batched(ctx, args, ws, local, g22))
     if ws == 1:
         res.update(extras_serving(ctx, args, local, g22))
@@ -677,6 +681,11 @@ def serve_stream(graphs, n, rate_qps, seed=7):
     return kinds, which, srcs, arrive
 
 
+def _progress(msg):
+    """One progress line on stderr (the JSON result goes to stdout)."""
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
+
+
 def _pct(lat):
     return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "p99.9_ms": float(np.percentile(lat, 99.9))}
@@ -706,6 +715,8 @@ def serve_plain(ctx, dgs, prios, stream, dev, hasher=None):
             ctx.mis_into(dgs[w], prios[w], mis_out[w])
         ctx.synchronize()
         lat[i] = (time.perf_counter() - t0 - arrive[i]) * 1e3
+        if i % 20000 == 19999:
+            _progress(f"plain: {i + 1} done")
         if hasher is not None:  # on the library's stream, before the buffer is reused
             hasher.put_now(i, mis_out[w] if k == 2 else outs[w])
     total = time.perf_counter() - t0
@@ -781,6 +792,8 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None):
         now = time.perf_counter() - t0
         late[i] = (now - arrive[i]) * 1e3
         owner[srv.submit(gids[w], k, s, row)] = (i, row, pool)
+        if i % 20000 == 19999:
+            _progress(f"server: {i + 1} submitted, {i + 1 - len(owner)} completed")
     while owner:
         drain(True)
     total = time.perf_counter() - t0
@@ -805,17 +818,19 @@ def extras_serving(ctx, args, local, g22):
     graphs = [ap.gen_rmat(16, 16, 16, 3), ap.gen_rmat(18, 16, 18, 3), ap.gen_rmat(20, 16, 2, 3), g22]
     dgs = [ap.DeviceGraph(g, dev) for g in graphs]
     prios = [torch.from_numpy(ap.mt19937_u32(4, g.m).view(np.int32)).to(dev) for g in graphs]
-    n = SERVE_QUERIES
+    n = args.serve_queries
     m_max = max(g.m for g in graphs)
     sat = serve_stream(graphs, n, 0.0)
     serve_plain(ctx, dgs, prios, serve_stream(graphs, 50, 0.0), dev)  # warm-up
     ref = RowHasher(ctx, m_max, n, dev)
+    _progress(f"serving: plain path, {n} queries")
     lat_p, tot_p = serve_plain(ctx, dgs, prios, sat, dev, ref)
     ref_h = ref.result()
     plain_qps = n / tot_p
     hctx = ap.Context(local)  # the server leg's checksums run on torch's current stream
 
     def run_server(stream):
+        _progress("serving: server")
         h = RowHasher(hctx, m_max, n, dev, ref.coef)
         lat_s, tot_s, st = serve_server(graphs, stream, dev, h)
         return lat_s, tot_s, st, int((h.result() == ref_h).sum())
@@ -833,6 +848,7 @@ def extras_serving(ctx, args, local, g22):
         rate = mult * plain_qps
         stream = serve_stream(graphs, n, rate)
         lat_s, tot_s, st, same = run_server(stream)
+        _progress(f"serving: plain path at {rate:.0f} queries/s")
         lat_p, tot_p = serve_plain(ctx, dgs, prios, stream, dev)
         res["serving"][f"poisson_{mult}x_plain_rate"] = {
             "rate_qps": rate, "server": dict(_pct(lat_s), qps=n / tot_s),
@@ -842,7 +858,9 @@ def extras_serving(ctx, args, local, g22):
     words = ap.mt19937_u32(8, n).astype(np.int64)
     bstream = (np.zeros(n, dtype=int), np.full(n, 3), words % graphs[3].m, np.zeros(n))
     bref = RowHasher(ctx, m_max, n, dev, ref.coef)
+    _progress("serving: BFS-only stream, plain path")
     lat_p, tot_p = serve_plain(ctx, dgs, prios, bstream, dev, bref)
+    _progress("serving: BFS-only stream, server")
     bref_h = bref.result()
     h = RowHasher(hctx, m_max, n, dev, ref.coef)
     lat_s, tot_s, st = serve_server(graphs, bstream, dev, h)
@@ -864,6 +882,8 @@ def main():
     ap_.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap_.add_argument("--no-extra", action="store_true")
     ap_.add_argument("--no-cpu-baseline", action="store_true")
+    ap_.add_argument("--serve-queries", type=int, default=SERVE_QUERIES,
+                     help="length of the serving streams (default: the config's 100,000)")
     ap_.add_argument("--only-extra", choices=["traversal", "spgemm_tc", "build", "batched", "serving"], default=None,
                      help="run one extra leg alone and print its JSON (no headline line)")
     args = ap_.parse_args()

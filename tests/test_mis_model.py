@@ -2,22 +2,22 @@
 the oracle's set (the greedy MIS in descending (priority, id) order) on every schedule, and
 models with a planted mistake do not.
 
-Modelled at the level that matters for correctness (mis_kernel): each undecided vertex keeps
-a scan position (the neighbour blocking it). Phase A re-checks the blocker; a vertex whose
-blocker went out (or that has none yet) scans the rest of its row. In phase B the vertices
-that joined last round write "out" into their neighbours while, interleaved at random with
-those writes, the scans read their neighbours' states in tiles of 1-3 edges, each tile
-flushing the least stop it saw into the vertex's `first` after its own reads. Phase C lets a
-scanned vertex with no stop join and gives one with a stop its new blocker. No GPU is
-involved."""
+Modelled at the level that matters for correctness (mis_kernel): vertices without
+neighbours join at once; each undecided vertex keeps a scan position (the neighbour
+blocking it). A round first lets the vertices that joined last round write "out" into their
+neighbours (phase P, complete before the scans start); then every undecided vertex, in
+steps interleaved at random with every other vertex's steps: leaves if it is out, waits if
+its blocker is still undecided (or in), else scans the rest of its row in chunks of 1-3
+neighbours, stopping at the first that outranks it and is not out, and then decides at
+once -- joining (state in, read by the others' later steps) when it found no stop. No GPU
+is involved."""
 import numpy as np
 import pytest
 
 import oracle
 from test_batch_sssp_model import _random_graph
 
-UNDECIDED, IN, OUT, SCAN = 0, 1, 2, 3
-INF = 1 << 60
+UNDECIDED, IN, OUT = 0, 1, 2
 
 
 def _outranks(pu, u, pv, v):
@@ -28,80 +28,59 @@ def _run_model(rp, ci, prio, rng, mistake=None):
     n = len(rp) - 1
     state = np.full(n, UNDECIDED)
     pos = np.array([int(rp[v]) - 1 for v in range(n)], dtype=np.int64)
-    first = np.full(n, INF, dtype=np.int64)
-    queue = [(v, False) for v in range(n)]  # (vertex, joined last round)
+    queue = []
+    for v in range(n):
+        if rp[v + 1] > rp[v]:
+            queue.append((v, False))
+        else:
+            state[v] = IN
     for _ in range(n + 3):
         if not queue:
             return state
-        # phase A
-        segs = []
+        # phase P
         for v, joined in queue:
-            r0, r1 = int(rp[v]), int(rp[v + 1])
             if joined:
-                segs.append((v, True, r0, r1))
-                continue
+                for e in range(int(rp[v]), int(rp[v + 1])):
+                    if int(ci[e]) != v:
+                        state[int(ci[e])] = OUT
+        # phase S: each undecided vertex is a generator of steps; run them interleaved
+        def steps(v):
+            if state[v] != UNDECIDED:
+                yield None
+                return
+            r0, r1 = int(rp[v]), int(rp[v + 1])
             p = int(pos[v])
-            scan = p < r0 or state[int(ci[p])] == OUT
-            if mistake == "skip_undecided_blocker" and p >= r0 and state[int(ci[p])] == UNDECIDED:
-                scan = True
-            if scan:
-                state[v] = SCAN
-                segs.append((v, False, p + 1, r1))
-        # phase B: push writes and scan tiles, interleaved at random
-        events = []
-        tiles = []
-        for v, joined, e0, e1 in segs:
-            e = e0
-            while e < e1:
+            if p >= r0 and state[int(ci[p])] != OUT and mistake != "skip_undecided_blocker":
+                nxt.append((v, False))  # still blocked
+                yield None
+                return
+            e = p + 1
+            stop = -1
+            while e < r1 and stop < 0:
                 k = int(rng.integers(1, 4))
-                edges = list(range(e, min(e + k, e1)))
-                e += k
-                if joined:
-                    for x in edges:
-                        events.append(("push", v, x))
-                else:
-                    tiles.append([v, edges, INF])
-                    t = len(tiles) - 1
-                    events.append(("read", t, None))
-                    events.append(("flush", t, None))
-        pending = set()
-        done_read = set()
-        for k in rng.permutation(len(events)):
-            kind, a, b = events[k]
-            if kind == "push":
-                u = int(ci[b])
-                if u != a:
-                    state[u] = OUT
-            elif kind == "read":
-                v, edges, _ = tiles[a]
-                for x in edges:
+                for x in range(e, min(e + k, r1)):
                     u = int(ci[x])
                     if u != v and state[u] != OUT and _outranks(prio[u], u, prio[v], v):
-                        tiles[a][2] = min(tiles[a][2], x)
-                done_read.add(a)
-                if a in pending:
-                    pending.discard(a)
-                    first[v] = min(first[v], tiles[a][2])
-            elif a in done_read:
-                first[tiles[a][0]] = min(first[tiles[a][0]], tiles[a][2])
-            else:
-                pending.add(a)
-        # phase C
-        nxt = []
-        for v, joined in queue:
-            if joined:
-                continue
-            if state[v] == UNDECIDED:
+                        stop = x
+                        break
+                e += k
+                yield None
+            if stop >= 0 and mistake != "join_despite_stop":
+                pos[v] = stop
                 nxt.append((v, False))
-            elif state[v] == SCAN:
-                if first[v] == INF or mistake == "join_despite_stop":
-                    state[v] = IN
-                    nxt.append((v, True))
-                else:
-                    pos[v] = first[v]
-                    first[v] = INF
-                    state[v] = UNDECIDED
-                    nxt.append((v, False))
+            else:
+                state[v] = IN
+                nxt.append((v, True))
+            yield None
+
+        nxt = []
+        gens = [steps(v) for v, joined in queue if not joined]
+        while gens:
+            k = int(rng.integers(0, len(gens)))
+            try:
+                next(gens[k])
+            except StopIteration:
+                gens.pop(k)
         queue = nxt
     raise AssertionError("no fixed point")
 
