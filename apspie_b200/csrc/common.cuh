@@ -37,7 +37,6 @@ struct TravCtl {
     long long edges_component;
     long long vertices_reached;
     long long aux[4];    // kernel-specific counters
-    int claim;           // grid-wide tile counter of an expansion phase (zeroed before it)
     int tl_count;        // phase timeline: block 0 stamps every grid barrier it passes
     int tl_site[kTimeline];
     unsigned long long tl_ns[kTimeline];

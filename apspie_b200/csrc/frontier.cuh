@@ -56,7 +56,6 @@ struct ExpandSmem {
     int base[kMaxGrid + 1];  // exclusive prefix of chunk totals
     int tsplit[BATCH + 1];   // merge-path split of each warp tile of the current batch
     int next_tile;           // tiles of the batch handed out so far (warps take them in turn)
-    int claim_base;          // first tile of the chunk this block claimed (grid-wide claiming)
     int scan_tmp[33];
     Warp w[NWARP];
 };
@@ -159,15 +158,11 @@ __device__ __forceinline__ int frontier_merge_path(long long diag, int nf, int E
 // entries k[]); post(ne, ws) runs after the tile's edges (per-entry flushes). All three
 // are called by every lane of the warp, so they may use warp collectives. DYN: warps claim
 // the tiles of their block's batch in turn (else tile i goes to warp i % NWARP).
-// claim == nullptr: every block owns a contiguous run of tiles. Otherwise blocks claim
-// chunks of 2 * NWARP consecutive tiles from the grid-wide counter *claim (zero when the
-// phase starts) until none is left, so that blocks whose tiles were cheap take more and
-// no block idles at the phase's end while another still has a long run to go.
 template <int BLOCK, int VT, bool EXTRA, bool DYN = true, class Load, class Op, class Post>
 __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__restrict__ loc_off,
                                                 const int *__restrict__ rs,
                                                 ExpandSmem<BLOCK, VT, EXTRA> &sm, Load load, Op op,
-                                                Post post, VGrid vg = hw_grid(), int *claim = nullptr) {
+                                                Post post, VGrid vg = hw_grid()) {
     using S = ExpandSmem<BLOCK, VT, EXTRA>;
     constexpr int WT = S::WT;
     constexpr int NWARP = S::NWARP;
@@ -265,210 +260,10 @@ __device__ __forceinline__ void frontier_expand(int nf, int E, const int *__rest
         }
         __syncthreads();
     };
-    if (claim == nullptr) {
-        const long long per = (ntiles + G - 1) / G;
-        const long long t_begin = static_cast<long long>(vg.id) * per;
-        const long long t_end = t_begin + per < ntiles ? t_begin + per : ntiles;
-        for (long long tb = t_begin; tb < t_end; tb += BATCH)
-            run_batch(tb, tb + BATCH < t_end ? tb + BATCH : t_end);
-    } else {
-        constexpr int CH = 2 * NWARP;
-        for (;;) {
-            if (threadIdx.x == 0) sm.claim_base = atomicAdd(claim, CH);
-            __syncthreads();
-            const long long tb = sm.claim_base;
-            if (tb >= ntiles) break;
-            run_batch(tb, tb + CH < ntiles ? tb + CH : ntiles);  // ends with __syncthreads
-        }
-        __syncthreads();  // every thread has read claim_base before it is reused
-    }
-}
-
-// ---------------------------------------------------------------------------------
-// Phase B with the next tile's entries staged asynchronously.
-//
-// A warp tile's entry data (scanned offset, row start, one payload word per entry) sit in
-// consecutive places of three arrays. Here a warp copies them for its NEXT tile into shared
-// memory with 16-byte cp.async.cg copies (L2 only: the arrays are rewritten every
-// iteration, so L1 could hold an old line) before it runs the operation on its current
-// tile, and waits for them only after that: the staging latency hides behind the current
-// tile's neighbour loads. Copies start at the 4-entry boundary at or below the tile's first
-// entry (16-byte aligned, as cp.async requires), so the staged arrays are offset by
-// sh = jb % 4; the entry labels handed to the operation include that offset, so
-// ws.rs[kk], ws.aux[kk] read the right slots. The copies may read up to three entries past
-// the last one: the arrays live in the context's arena, whose buffers are padded.
-template <int WT>
-struct PipeSlice {
-    alignas(16) int off[WT + 8];
-    alignas(16) int rs[WT + 8];
-    alignas(16) int aux[WT + 8];
-};
-
-template <int BLOCK, int VT>
-struct PipeSmem {
-    static constexpr int NWARP = BLOCK / 32;
-    static constexpr int WT = 32 * VT;
-    static constexpr int BATCH = BLOCK;
-    using Warp = PipeSlice<WT>;
-    static constexpr int QCAP = 128;
-    int qbuf[NWARP][2][QCAP];
-    int base[kMaxGrid + 1];
-    int tsplit[BATCH + 1];
-    int next_tile;
-    int claim_base;
-    int scan_tmp[33];
-    int seg[NWARP][WT];
-    Warp w[2][NWARP];
-};
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-// Same contract as frontier_expand, with payload[j] staged into ws.aux (nullptr: none) in
-// place of a load hook, and post(ne, sh, ws) told the staged slots' offset.
-template <int BLOCK, int VT, class Op, class Post>
-__device__ __forceinline__ void frontier_expand_pipe(int nf, int E, const int *__restrict__ loc_off,
-                                                     const int *__restrict__ rs, const int *__restrict__ payload,
-                                                     PipeSmem<BLOCK, VT> &sm, Op op, Post post,
-                                                     VGrid vg = hw_grid(), int *claim = nullptr) {
-    using S = PipeSmem<BLOCK, VT>;
-    constexpr int WT = S::WT;
-    constexpr int NWARP = S::NWARP;
-    constexpr int BATCH = S::BATCH;
-    const int G = vg.n;
-    const int C = (nf + G - 1) / G;
-    const long long total = static_cast<long long>(nf) + E;
-    const long long ntiles = (total + WT - 1) / WT;
-    const int lane = threadIdx.x & 31;
-    const int wid = threadIdx.x >> 5;
-    int *seg = sm.seg[wid];
-    // issue the copies of tile `tile`'s entries into buffer b
-    auto stage = [&](long long tile, long long tb, int b) {
-        const int a0 = sm.tsplit[tile - tb];
-        const int a1 = sm.tsplit[tile - tb + 1];
-        const int jb = a0 > 0 ? a0 - 1 : 0;
-        const int j0 = jb & ~3;
-        const int nch = (a1 - j0 + 3) >> 2;  // 16-byte chunks covering [j0, a1)
-        typename S::Warp &ws = sm.w[b][wid];
-        for (int c = lane; c < nch; c += 32) {
-            cp_async16(ws.off + 4 * c, loc_off + j0 + 4 * c);
-            cp_async16(ws.rs + 4 * c, rs + j0 + 4 * c);
-            if (payload) cp_async16(ws.aux + 4 * c, payload + j0 + 4 * c);
-        }
-        cp_async_commit();
-    };
-    // tile `tile` staged in buffer b: wait for its copies, finish the offsets, label the
-    // edge slots
-    struct Prep {
-        bool valid[VT];
-        int kk[VT], idx[VT];
-        int ne, sh;
-    };
-    auto prep = [&](long long tile, long long tb, int b) {
-        typename S::Warp &ws = sm.w[b][wid];
-        Prep p;
-        const long long d0 = tile * WT;
-        const long long d1 = d0 + WT < total ? d0 + WT : total;
-        const int a0 = sm.tsplit[tile - tb];
-        const int a1 = sm.tsplit[tile - tb + 1];
-        const int e0 = static_cast<int>(d0 - a0);
-        const int e1 = static_cast<int>(d1 - a1);
-        const int jb = a0 > 0 ? a0 - 1 : 0;
-        const int sh = jb & 3;
-        p.ne = a1 - jb;
-        p.sh = sh;
-        cp_async_wait_all();
-        __syncwarp();
-        for (int k = lane; k < p.ne; k += 32) ws.off[k + sh] += sm.base[(jb + k) / C];
-        __syncwarp();
-        const int tcount = static_cast<int>(d1 - d0);
-        const int diag = lane * VT;
-        if (diag < tcount) {
-            const int acount = a1 - a0, bcount = e1 - e0;
-            int lo = diag - bcount > 0 ? diag - bcount : 0;
-            int hi = diag < acount ? diag : acount;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (ws.off[a0 + mid - jb + sh] <= e0 + diag - 1 - mid)
-                    lo = mid + 1;
-                else
-                    hi = mid;
-            }
-            int ja = a0 + lo, eb = e0 + diag - lo;
-            int cur = ja - 1 - jb + sh;
-            const int end = diag + VT < tcount ? diag + VT : tcount;
-            for (int it = diag; it < end; ++it) {
-                if (ja < a1 && ws.off[ja - jb + sh] <= eb) {
-                    cur = ja - jb + sh;
-                    ++ja;
-                } else {
-                    seg[eb - e0] = cur;
-                    ++eb;
-                }
-            }
-        }
-        __syncwarp();
-        const int ned = e1 - e0;
-#pragma unroll
-        for (int r = 0; r < VT; ++r) {
-            const int el = r * 32 + lane;
-            p.valid[r] = el < ned;
-            p.kk[r] = 0;
-            p.idx[r] = 0;
-            if (p.valid[r]) {
-                p.kk[r] = seg[el];
-                p.idx[r] = ws.rs[p.kk[r]] + (e0 + el - ws.off[p.kk[r]]);
-            }
-        }
-        return p;
-    };
-    auto run_batch = [&](long long tb, long long te) {
-        for (int s = threadIdx.x; s <= te - tb; s += BLOCK) {
-            long long d = (tb + s) * WT;
-            if (d > total) d = total;
-            sm.tsplit[s] = frontier_merge_path(d, nf, E, loc_off, sm.base, C);
-        }
-        if (threadIdx.x == 0) sm.next_tile = NWARP;
-        __syncthreads();
-        long long tile = tb + wid;
-        int b = 0;
-        if (tile < te) stage(tile, tb, b);
-        while (tile < te) {
-            int nt = 0;
-            if (lane == 0) nt = atomicAdd(&sm.next_tile, 1);
-            const long long nxt = tb + __shfl_sync(0xffffffffu, nt, 0);
-            const Prep p = prep(tile, tb, b);     // waits for this tile's copies
-            if (nxt < te) stage(nxt, tb, b ^ 1);  // the next tile's copies fly during the op
-            op(p.valid, p.kk, p.idx, sm.w[b][wid]);
-            __syncwarp();
-            post(p.ne, p.sh, sm.w[b][wid]);
-            tile = nxt;
-            b ^= 1;
-            __syncwarp();
-        }
-        __syncthreads();
-    };
-    if (claim == nullptr) {
-        const long long per = (ntiles + G - 1) / G;
-        const long long t_begin = static_cast<long long>(vg.id) * per;
-        const long long t_end = t_begin + per < ntiles ? t_begin + per : ntiles;
-        for (long long tb = t_begin; tb < t_end; tb += BATCH)
-            run_batch(tb, tb + BATCH < t_end ? tb + BATCH : t_end);
-    } else {
-        constexpr int CH = 2 * NWARP;
-        for (;;) {
-            if (threadIdx.x == 0) sm.claim_base = atomicAdd(claim, CH);
-            __syncthreads();
-            const long long tb = sm.claim_base;
-            if (tb >= ntiles) break;
-            run_batch(tb, tb + CH < ntiles ? tb + CH : ntiles);
-        }
-        __syncthreads();
-    }
+    const long long per = (ntiles + G - 1) / G;
+    const long long t_begin = static_cast<long long>(vg.id) * per;
+    const long long t_end = t_begin + per < ntiles ? t_begin + per : ntiles;
+    for (long long tb = t_begin; tb < t_end; tb += BATCH) run_batch(tb, tb + BATCH < t_end ? tb + BATCH : t_end);
 }
 
 }  // namespace apspie

@@ -27,9 +27,11 @@
 // A free slot takes the (graph, kind) whose oldest waiting request is oldest. A launch is
 // admitted only if resident graphs + the slots' scratch + the launch's own growth fit the
 // budget; otherwise it shrinks (fewer requests, or fewer engine query slots) or waits for
-// a running launch to finish. An engine stops admitting (finishes its queries and leaves
-// the slot) once other work has waited for a slot longer than it has run, or when its
-// waiting requests outgrow its query slots (it is relaunched with more). Launches whose
+// a running launch to finish. Single-source requests run at most kSingleSourcePerLaunch per
+// slot launch. An engine stops admitting (finishes its queries and leaves the slot) once
+// other work has waited for a slot longer than it has run, or when its waiting requests
+// outgrow its query slots (it is relaunched with more), but only after kEngineMinRun; an
+// engine started while nothing else runs or waits takes the whole device. Launches whose
 // device-side wait ran out (a persistent grid that could not be co-resident, e.g. on a
 // GPU shared with other work) are retried with half the grid. Every answer is computed by
 // the same kernels as the plain path, so it is identical whether the request ran alone or
@@ -96,7 +98,11 @@ struct Slot {
     int32_t *d_src = nullptr;  // device copy of a batch's sources
     int src_cap = 0;
     int retries = 0;
+    int share = 1;  // the slot's persistent grids take 1/share of the device (doubled on a timeout)
 };
+
+constexpr int kSingleSourcePerLaunch = 16;
+constexpr std::chrono::microseconds kEngineMinRun(5000);
 
 // Rows answered without a traversal: sources without edges.
 constexpr int kTrivialMax = 64;
@@ -219,7 +225,7 @@ void finish_batch(apspie_server *s, Slot &sl, std::map<std::pair<int, int>, std:
     if (status == APSPIE_OK) sl.retries = 0;
     if (status == APSPIE_ERR_TIMEOUT && sl.retries < 3) {
         // a persistent grid did not get all of its blocks at once: retry on half the grid
-        sl.ctx->grid_share *= 2;
+        sl.share *= 2;
         ++sl.retries;
         auto &q = pending[{sl.batch.front().graph, sl.kind}];
         for (auto it = sl.batch.rbegin(); it != sl.batch.rend(); ++it) q.push_front(*it);
@@ -397,7 +403,7 @@ void engine_ended(apspie_server *s, Slot &sl, std::map<std::pair<int, int>, std:
         back.insert(back.end(), taken.begin(), taken.end());
         std::sort(back.begin(), back.end(), [](const Request &a, const Request &b) { return a.ticket < b.ticket; });
         if (st == APSPIE_ERR_TIMEOUT && sl.retries < 3) {
-            sl.ctx->grid_share *= 2;
+            sl.share *= 2;
             ++sl.retries;
         } else {
             fail = true;
@@ -510,9 +516,18 @@ void worker_loop(apspie_server *s) {
                 break;  // wait for memory to free up
             }
             sl.busy = true;
+            sl.ctx->grid_share = sl.share;
             if (kind == APSPIE_QUERY_BFS && batched(kind, n, mb)) {
                 const int W = bfs_engine_words(n);
                 feed_engine(s, gi, best->second);
+                // an engine that starts while nothing else runs or waits takes the whole
+                // device; work arriving later waits for it to drain (it is drained for such
+                // work after kEngineMinRun)
+                bool alone = true;
+                for (auto &other : s->slots) alone &= &other == &sl || !other.busy;
+                for (auto &kv : pending)
+                    alone &= kv.second.empty() || (kv.first.first == gi && kv.first.second == APSPIE_QUERY_BFS);
+                if (alone) sl.ctx->grid_share = std::max(1, sl.share / static_cast<int>(s->slots.size()));
                 const apspie_status st = bfs_engine_launch(sl.ctx, &g.view, W, g.eng);
                 if (st != APSPIE_OK) {
                     // the launch never started: every request in its ring fails
@@ -539,6 +554,9 @@ void worker_loop(apspie_server *s) {
                 s->st.peak_bytes = std::max<int64_t>(s->st.peak_bytes, static_cast<int64_t>(held + need));
                 continue;
             }
+            // requests that run one single-source launch each: a few per slot launch, so
+            // that slots turn over (a scale-22 SSSP takes about 2 ms)
+            if (!batched(kind, n, mb) && kind != APSPIE_QUERY_MIS) n = std::min(n, kSingleSourcePerLaunch);
             if (kind == APSPIE_QUERY_BFS) n = std::min(n, static_cast<int>(best->second.size()));
             sl.kind = kind;
             sl.engine_graph = -1;
@@ -566,16 +584,18 @@ void worker_loop(apspie_server *s) {
                 for (auto &kv : pending)
                     if (!kv.second.empty() && !(kv.first.second == APSPIE_QUERY_BFS && &s->graphs[kv.first.first] == &g))
                         oldest = std::min(oldest, kv.second.front().t_submit);
-                // other work may wait as long as the engine has run, at least 2 ms, at most 50 ms
+                // other work may wait as long as the engine has run, at least 2 ms, at most
+                // 50 ms; an engine always runs kEngineMinRun first (its first levels)
                 const auto ran = std::chrono::duration_cast<std::chrono::microseconds>(now - g.eng_t0);
                 const auto allow = std::max(std::chrono::microseconds(2000),
                                             std::min(std::chrono::microseconds(50000), ran));
-                drain = now - oldest > allow;
+                drain = ran >= kEngineMinRun && now - oldest > allow;
             }
             const int slots = 32 * g.eng_W;
             auto it = pending.find({static_cast<int>(&g - s->graphs.data()), APSPIE_QUERY_BFS});
             const size_t backlog = bfs_engine_waiting(g.eng) + (it == pending.end() ? 0 : it->second.size());
-            if (slots < s->max_batch && backlog > static_cast<size_t>(2 * slots)) drain = true;
+            if (slots < s->max_batch && backlog > static_cast<size_t>(2 * slots) && now - g.eng_t0 >= kEngineMinRun)
+                drain = true;
             if (drain) {
                 bfs_engine_set_accept(g.eng, 0);
                 g.eng_accepting = false;
@@ -623,6 +643,7 @@ apspie_status apspie_server_create(int device, int64_t memory_budget_bytes, int3
         // when their kernels differ in footprint. (A grid whose blocks could not all be
         // resident ends its wait at a grid barrier with APSPIE_ERR_TIMEOUT; the launch is
         // then retried on half the grid.)
+        sl.share = num_slots;
         sl.ctx->grid_share = num_slots;
     }
     *out = s;

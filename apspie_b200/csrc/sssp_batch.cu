@@ -36,9 +36,6 @@ namespace {
 #ifndef APSPIE_SB_VT
 #define APSPIE_SB_VT 2
 #endif
-#ifndef APSPIE_SB_STAGE
-#define APSPIE_SB_STAGE 1  // 1: broadcast each edge's fields with one shared-memory load, reuse u's labels
-#endif
 constexpr int kSbBlock = 256;
 constexpr int kSbVT = APSPIE_SB_VT;
 constexpr int kSbUnroll = APSPIE_SB_UNROLL;  // edges whose label reads a warp issues together
@@ -73,9 +70,6 @@ struct RowOfPacked {
 
 __global__ void __launch_bounds__(kSbBlock, APSPIE_SB_MINB) sssp_batch_kernel(SbArgs a) {
     __shared__ SbSmem sm;
-    // each lane's edges (target entry, weight, source entry, changed bits), read back by
-    // the whole warp with one 16-byte broadcast load per edge
-    __shared__ int4 s_edge[APSPIE_SB_STAGE ? kSbBlock / 32 : 1][kSbVT][32];
     timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
     const int gtid = blockIdx.x * kSbBlock + threadIdx.x;
@@ -177,22 +171,11 @@ __global__ void __launch_bounds__(kSbBlock, APSPIE_SB_MINB) sssp_batch_kernel(Sb
                     }
                 }
                 unsigned *lab_l = lab + lane;  // this lane's query in every label line
-                if (APSPIE_SB_STAGE) {
-#pragma unroll
-                    for (int r = 0; r < kSbVT; ++r)
-                        s_edge[APSPIE_SB_STAGE ? wid : 0][r][lane] =
-                            make_int4(tv[r], we[r], eu[r], static_cast<int>(bits[r]));
-                    __syncwarp();
-                }
 #pragma unroll
                 for (int r = 0; r < kSbVT; ++r) {
                     const unsigned vmask = __ballot_sync(0xffffffffu, bits[r] != 0u);
                     if (vmask == 0u) continue;
                     unsigned mine = 0u;  // improved queries of this lane's edge r
-                    // consecutive edges mostly leave the same entry: its label line, read once
-                    // in this pass (coherently, so never older than the pass), is reused
-                    int pu = -1;
-                    unsigned pb = 0u, pdu = 0u;
 #pragma unroll 1
                     for (int l0 = 0; l0 < 32; l0 += kSbUnroll) {
                         if (((vmask >> l0) & ((1u << kSbUnroll) - 1u)) == 0u) continue;
@@ -202,29 +185,14 @@ __global__ void __launch_bounds__(kSbBlock, APSPIE_SB_MINB) sssp_batch_kernel(Sb
 #pragma unroll
                         for (int t = 0; t < kSbUnroll; ++t) {
                             const int l = l0 + t;
-                            int u;
-                            unsigned b;
-                            if (APSPIE_SB_STAGE) {
-                                const int4 e4 = s_edge[APSPIE_SB_STAGE ? wid : 0][r][l];
-                                ev[t] = e4.x;
-                                wl[t] = e4.y;
-                                u = e4.z;
-                                b = static_cast<unsigned>(e4.w);
-                            } else {
-                                ev[t] = __shfl_sync(0xffffffffu, tv[r], l);
-                                wl[t] = __shfl_sync(0xffffffffu, we[r], l);
-                                u = __shfl_sync(0xffffffffu, eu[r], l);
-                                b = __shfl_sync(0xffffffffu, bits[r], l);
-                            }
+                            ev[t] = __shfl_sync(0xffffffffu, tv[r], l);
+                            wl[t] = __shfl_sync(0xffffffffu, we[r], l);
+                            const int u = __shfl_sync(0xffffffffu, eu[r], l);
+                            const unsigned b = __shfl_sync(0xffffffffu, bits[r], l);
                             act[t] = (b >> lane) & 1u;
                             // coherent reads: a label lowered since the entry was queued must be
                             // seen (its change bit was consumed in phase A)
-                            if (!APSPIE_SB_STAGE || u != pu || b != pb) {  // the same in every lane
-                                pdu = act[t] ? __ldcg(lab_l + static_cast<size_t>(u) * 32) : 0u;
-                                pu = u;
-                                pb = b;
-                            }
-                            du[t] = pdu;
+                            du[t] = act[t] ? __ldcg(lab_l + static_cast<size_t>(u) * 32) : 0u;
                             dv[t] = act[t] ? __ldcg(lab_l + static_cast<size_t>(ev[t]) * 32) : 0u;
                         }
                         // an improvement over the label just read is reported without waiting

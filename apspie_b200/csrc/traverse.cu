@@ -30,12 +30,6 @@ namespace {
 #ifndef APSPIE_SSSP_PREREAD
 #define APSPIE_SSSP_PREREAD 1
 #endif
-#ifndef APSPIE_SSSP_CLAIM
-#define APSPIE_SSSP_CLAIM 0  // 1: blocks claim expansion tiles from a grid-wide counter
-#endif
-#ifndef APSPIE_TRAV_CLAIM
-#define APSPIE_TRAV_CLAIM 0  // the same for the BFS push and MIS expansions
-#endif
 
 
 constexpr int kBlock = 256;
@@ -46,22 +40,13 @@ using BfsSmem = ExpandSmem<kBlock, kVT, false>;
 using BfsSlice = BfsSmem::Warp;
 constexpr int kSsspVT = APSPIE_SSSP_VT;
 constexpr int kSsspPA = 4;  // frontier entries per thread per phase-A step
-#ifndef APSPIE_SSSP_PIPE
-#define APSPIE_SSSP_PIPE 0  // 1: the expansion stages the next tile's entries with cp.async
-#endif
-#if APSPIE_SSSP_PIPE
-using SsspSmem = PipeSmem<kBlock, kSsspVT>;
-#else
 using SsspSmem = ExpandSmem<kBlock, kSsspVT, false>;
-#endif
 using SsspSlice = SsspSmem::Warp;
 using WQ = WarpQueue<Smem::QCAP>;
 
 struct NoPost {
     template <class S>
     __device__ void operator()(int, S &) const {}
-    template <class S>
-    __device__ void operator()(int, int, S &) const {}
 };
 
 constexpr int kInf = 0x7fffffff;
@@ -183,10 +168,7 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
                                      atomicOr(fbc + (v >> 5), 1u << (v & 31));
                                      return deg;
                                  });
-        if (gtid == 0) {
-            *qlen_next = 0;
-            a.ctl->claim = 0;
-        }
+        if (gtid == 0) *qlen_next = 0;
         if (!grid_barrier(a.ctl, a.sticky, kSiteBfs + 1)) return;
 
         const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
@@ -233,7 +215,7 @@ __global__ void __launch_bounds__(kBlock) bfs_kernel(BfsArgs a) {
                         wq.push(fresh[r], v[r]);
                     }
                 },
-                NoPost(), hw_grid(), APSPIE_TRAV_CLAIM ? &a.ctl->claim : nullptr);
+                NoPost());
             wq.flush();
         } else {
             ++npull;
@@ -565,7 +547,6 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
             }
             if (threadIdx.x == 0) a.buf.chunk_sum[vg.id] = carry;
         }
-        if (APSPIE_SSSP_CLAIM && gtid == 0) a.ctl->claim = 0;
         if (!grid_barrier(a.ctl, a.sticky, kSiteSsspBarA, vg)) return;
         // every block has read this queue's length, base and histogram: reset them for the
         // iteration that fills this queue next
@@ -678,14 +659,9 @@ __device__ __forceinline__ void sssp_body(SsspArgs a, VGrid vg) {
                     wf.push(far[r], v[r]);
                 }
             };
-#if APSPIE_SSSP_PIPE
-        frontier_expand_pipe<kBlock, kSsspVT>(nf, E, a.buf.loc_off, a.buf.rs, snap, sm, relax, NoPost(), vg,
-                                              APSPIE_SSSP_CLAIM ? &a.ctl->claim : nullptr);
-#else
         frontier_expand<kBlock, kSsspVT, false>(
             nf, E, a.buf.loc_off, a.buf.rs, sm, [&](int jj, int k, SsspSlice &w) { w.aux[k] = __ldcg(snap + jj); },
-            relax, NoPost(), vg, APSPIE_SSSP_CLAIM ? &a.ctl->claim : nullptr);
-#endif
+            relax, NoPost(), vg);
         wn.flush();
         wf.flush();
         if (banded) {
@@ -811,9 +787,9 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_group_kernel(Ss
 // MIS
 // ================================================================================
 enum : unsigned char { kUndecided = 0, kIn = 1, kOut = 2 };
-constexpr int kJoinEntry = static_cast<int>(0x80000000u);  // queue entry: a vertex that joined
-constexpr int kMisGroup = 8;   // lanes that scan one vertex's row together
-constexpr int kMisChunks = 4;  // chunks of kMisGroup neighbours a group scans before handing on
+constexpr int kMisGroup = 4;    // lanes that scan one vertex's row together (phase S)
+constexpr int kMisChunks = 4;   // chunks of kMisGroup neighbours a group scans before handing on
+constexpr int kMisWarpChunks = 64;  // chunks of 32 neighbours a warp scans (phase L) before handing on
 
 struct MisArgs {
     int m, nnz;
@@ -823,19 +799,26 @@ struct MisArgs {
     unsigned char *member;
     int *member_i32;  // when set, the set is written here as int32 1/0 instead
     unsigned char *state;
-    int *pos;    // CSR index of the outranking neighbour that blocks the vertex (row start - 1: none yet)
-    int *longq;  // vertices whose scan continues past kMisGroup * kMisChunks neighbours this round
+    int *pos;     // CSR index of the outranking neighbour that blocks the vertex (row start - 1: none yet)
+    int *joined;  // the vertices that joined in the last round (they push next round)
+    int *longq;   // scans that go on past a group's share this round (one warp each)
+    int *longq2;  // scans that go on past a warp's share (one block each)
     TravBuffers buf;
     TravCtl *ctl;
     int *sticky;
 };
 
-struct RowOfMisEntry {
-    __device__ __forceinline__ int operator()(int e) const { return e & ~kJoinEntry; }
-};
-
 __device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v) {
     return pu > pv || (pu == pv && u > v);
+}
+
+// One neighbour of a scanning vertex v: does it decide anything (an outranking neighbour
+// that is not out: v's new blocker, or -- if in -- the vertex whose push knocks v out)?
+__device__ __forceinline__ bool mis_stop(const MisArgs &a, int idx, int v, unsigned pv) {
+    const int u = __ldg(a.col_ind + idx);
+    const unsigned pu = __ldg(a.prio + u);
+    const unsigned char su = __ldcg(a.state + u);
+    return u != v && su != kOut && outranks(pu, u, pv, v);
 }
 
 // Greedy MIS in descending (priority, id) order -- the set spmspvMis converges to
@@ -848,24 +831,23 @@ __device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v)
 // join while the vertex is undecided), and a neighbour once seen out or lower-ranked
 // stays so. So each undecided vertex keeps a scan position `pos`: every neighbour before
 // it is settled, and the neighbour at it is its current blocker (undecided, outranking).
-// A row is read about once over the whole run, and each scan stops at the first
-// neighbour that decides anything: about 1.5M neighbour reads for R-MAT scale 20's 31.4M
-// entries. Vertices without neighbours join at the start. Round r, over a queue holding
-// the undecided vertices and the vertices that joined in round r-1:
+// Each scan stops at the first neighbour that decides anything, so rows are read about
+// once over the whole run and mostly not to their end (about 6.8M of R-MAT scale 20's
+// 31.4M entries). Vertices without neighbours join at the start. Round r, over the queue
+// of undecided vertices and the list of vertices that joined in round r-1:
 //  phase A  row lengths of the joined vertices (merge-path scan);
-//  phase P  the joined vertices write out into their neighbours (merge-path expansion);
+//  phase P  they write out into their neighbours (merge-path expansion);
 //  phase S  each undecided vertex, by a group of kMisGroup lanes: out -> leaves; its
 //           blocker still undecided (or in: its push comes next round) -> waits; else it
-//           scans the rest of its row in chunks of kMisGroup, stopping at the first
-//           neighbour that outranks it and is not out (its new blocker); no such neighbour
-//           -> it joins (and is queued to push next round). After kMisChunks chunks without
-//           an end the vertex goes to the long list;
-//  phase L  (only when the long list is not empty) one block per listed vertex scans on to
-//           its stop or its row's end.
+//           scans on in chunks of kMisGroup and stops at the first neighbour that outranks
+//           it and is not out (its new blocker); no such neighbour -> it joins. After
+//           kMisChunks chunks without an end the vertex goes to the long list;
+//  phase L  (only when that list is not empty) one warp per vertex goes on in chunks of
+//           32, for up to kMisWarpChunks chunks; the rest (phase L2) one block each.
 // The pushes of a round are complete before its scans start, so a scan sees every
 // vertex knocked out so far; scans and joins of the same phase race only safely (a vertex
-// joins only if every outranking neighbour was seen out, and out is final). The set is
-// the greedy MIS whatever the timing.
+// joins only if every outranking neighbour was seen not to be, and out is final). The set
+// is the greedy MIS whatever the timing.
 __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
     __shared__ Smem sm;
     __shared__ int s_stop;
@@ -877,9 +859,10 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
     const int wid = threadIdx.x >> 5;
     const int m = a.m;
     const int *col = a.col_ind;
-    const unsigned *prio = a.prio;
     unsigned char *state = a.state;
-    int *l2len = &a.ctl->flen[0];
+    int *jlen = &a.ctl->flen[0];             // [2]: joined-list lengths, by round parity
+    int *l1len = reinterpret_cast<int *>(&a.ctl->aux[0]);
+    int *l2len = reinterpret_cast<int *>(&a.ctl->aux[1]);
     {
         WQ wq(sm.qbuf[wid][0], a.buf.q0, &a.ctl->qlen[0]);
         for (int base = blockIdx.x * kBlock; base < m; base += gstride) {
@@ -895,18 +878,22 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         }
         wq.flush();
     }
-    if (gtid == 0) a.ctl->qlen[1] = 0;
+    if (gtid == 0) {
+        a.ctl->qlen[1] = 0;
+        jlen[0] = jlen[1] = 0;
+    }
     if (!grid_barrier(a.ctl, a.sticky, kSiteMis)) return;
 
-    int cur = 0;
+    int cur = 0, jc = 0;
     long long expanded = 0, scanned = 0;
     int round = 0;
-    const int g8 = lane / kMisGroup, l8 = lane % kMisGroup;
-    const unsigned gmask = ((1u << kMisGroup) - 1u) << (g8 * kMisGroup);
+    const int gl = lane / kMisGroup, ll = lane % kMisGroup;
+    const unsigned gmask = ((1u << kMisGroup) - 1u) << (gl * kMisGroup);
     constexpr int kGroupsPerWarp = 32 / kMisGroup;
     for (;;) {
         const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
-        if (nf == 0) break;
+        const int nj = ld_volatile_i32(jlen + jc);
+        if (nf == 0 && nj == 0) break;
         if (round > m + 1) {
             if (gtid == 0) raise_error(a.ctl, a.sticky, APSPIE_ERR_NOT_CONVERGED, kSiteMisRoundCap);
             break;
@@ -915,12 +902,15 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         int *qc = cur ? a.buf.q1 : a.buf.q0;
         int *qn = cur ? a.buf.q0 : a.buf.q1;
         int *qlen_next = &a.ctl->qlen[cur ^ 1];
+        int *jlen_next = jlen + (jc ^ 1);
 
-        // phase A: row lengths of the joined vertices (undecided entries expand nothing)
-        frontier_phase_a<kBlock>(qc, nf, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum, sm.scan_tmp,
-                                 [](int, int e, int deg) { return (e & kJoinEntry) ? deg : 0; }, RowOfMisEntry{});
+        // phase A: row lengths of the joined vertices
+        frontier_phase_a<kBlock>(a.joined, nj, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum, sm.scan_tmp,
+                                 [](int, int, int deg) { return deg; });
         if (gtid == 0) {
             *qlen_next = 0;
+            *jlen_next = 0;
+            *l1len = 0;
             *l2len = 0;
         }
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 1)) return;
@@ -929,9 +919,9 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
         if (E > 0) {
             expanded += E;
+            const int *jl = a.joined;
             frontier_expand<kBlock, kVT, true, false>(
-                nf, E, a.buf.loc_off, a.buf.rs, sm,
-                [&](int j, int k, WarpSlice &ws) { ws.aux[k] = __ldcg(qc + j) & ~kJoinEntry; },
+                nj, E, a.buf.loc_off, a.buf.rs, sm, [&](int j, int k, WarpSlice &ws) { ws.aux[k] = __ldcg(jl + j); },
                 [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT], WarpSlice &ws) {
                     int u[kVT];
 #pragma unroll
@@ -944,43 +934,36 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
             if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 2)) return;
         }
 
-        // phase S: blocker checks, scans, decisions (kGroupsPerWarp vertices per warp)
+        // phase S: blocker checks, short scans and decisions, kGroupsPerWarp vertices a warp
         {
             WQ wq(sm.qbuf[wid][0], qn, qlen_next);
-            WQ wl(sm.qbuf[wid][1], a.longq, l2len);
+            WQ wj(sm.qbuf[wid][1], a.joined, jlen_next);
             const int gw = gtid >> 5, nw = gstride >> 5;
             for (int wb = gw * kGroupsPerWarp; wb < nf; wb += nw * kGroupsPerWarp) {
-                const int i = wb + g8;
-                const int e = i < nf ? __ldcg(qc + i) : kJoinEntry;
-                const int v = e & ~kJoinEntry;
+                const int i = wb + gl;
+                const int v = i < nf ? __ldcg(qc + i) : 0;
                 bool scanning = false, keep = false, joined = false, handed = false;
                 int start = 0, r1 = 0;
                 unsigned pv = 0;
-                if (!(e & kJoinEntry) && __ldcg(state + v) == kUndecided) {
+                if (i < nf && __ldcg(state + v) == kUndecided) {
                     const int r0 = __ldg(a.row_ptr + v);
                     r1 = __ldg(a.row_ptr + v + 1);
                     const int p = __ldcg(a.pos + v);
                     scanning = p < r0 || __ldcg(state + __ldg(col + p)) == kOut;
                     keep = !scanning;  // its blocker is undecided, or joined (and pushes next round)
                     start = p + 1;
-                    pv = __ldg(prio + v);
+                    pv = __ldg(a.prio + v);
                 }
                 int stop = -1;
                 bool done = !scanning;
 #pragma unroll
                 for (int c = 0; c < kMisChunks; ++c) {
-                    const int idx = start + c * kMisGroup + l8;
-                    bool st = false;
-                    if (!done && idx < r1) {
-                        const int u = __ldg(col + idx);
-                        const unsigned pu = __ldg(prio + u);
-                        const unsigned char su = __ldcg(state + u);
-                        st = u != v && su != kOut && outranks(pu, u, pv, v);
-                    }
+                    const int idx = start + c * kMisGroup + ll;
+                    const bool st = !done && idx < r1 && mis_stop(a, idx, v, pv);
                     const unsigned b = __ballot_sync(0xffffffffu, st) & gmask;
                     if (!done) {
                         if (b) {
-                            stop = start + c * kMisGroup + (__ffs(b) - 1 - g8 * kMisGroup);
+                            stop = start + c * kMisGroup + (__ffs(b) - 1 - gl * kMisGroup);
                             done = true;
                         } else if (start + (c + 1) * kMisGroup >= r1) {
                             joined = true;
@@ -989,45 +972,79 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                     }
                 }
                 if (scanning) {
-                    if (l8 == 0) scanned += min(r1, stop >= 0 ? stop + 1 : start + kMisChunks * kMisGroup) - start;
+                    if (ll == 0) scanned += min(r1, stop >= 0 ? stop + 1 : start + kMisChunks * kMisGroup) - start;
                     if (stop >= 0) {
                         keep = true;
-                        if (l8 == 0) a.pos[v] = stop;
+                        if (ll == 0) a.pos[v] = stop;
                     } else if (joined) {
-                        keep = true;
-                        if (l8 == 0) state[v] = kIn;
+                        if (ll == 0) state[v] = kIn;
                     } else {
                         handed = true;  // settled up to start + kMisChunks * kMisGroup - 1
-                        if (l8 == 0) a.pos[v] = start + kMisChunks * kMisGroup - 1;
+                        if (ll == 0) a.pos[v] = start + kMisChunks * kMisGroup - 1;
                     }
                 }
-                wq.push(keep && l8 == 0, joined ? (v | kJoinEntry) : v);
-                wl.push(handed && l8 == 0, v);
+                wq.push(keep && ll == 0, v);
+                wj.push(joined && ll == 0, v);
+                if (handed && ll == 0) a.longq[atomicAdd(l1len, 1)] = v;
             }
             wq.flush();
-            wl.flush();
+            wj.flush();
         }
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 3)) return;
 
-        // phase L: the long scans, one block per vertex
-        const int nl = ld_volatile_i32(l2len);
-        if (nl > 0) {
-            for (int k = blockIdx.x; k < nl; k += G) {
+        // phase L: longer scans, one warp per vertex
+        const int n1 = ld_volatile_i32(l1len);
+        if (n1 > 0) {
+            WQ wq(sm.qbuf[wid][0], qn, qlen_next);
+            WQ wj(sm.qbuf[wid][1], a.joined, jlen_next);
+            const int gw = gtid >> 5, nw = gstride >> 5;
+            for (int k = gw; k < n1; k += nw) {
                 const int v = __ldcg(a.longq + k);
                 const int r1 = __ldg(a.row_ptr + v + 1);
                 const int start = __ldcg(a.pos + v) + 1;
-                const unsigned pv = __ldg(prio + v);
+                const unsigned pv = __ldg(a.prio + v);
+                int stop = -1, c = 0;
+                for (; c < kMisWarpChunks && start + 32 * c < r1; ++c) {
+                    const int idx = start + 32 * c + lane;
+                    const unsigned b = __ballot_sync(0xffffffffu, idx < r1 && mis_stop(a, idx, v, pv));
+                    if (b) {
+                        stop = start + 32 * c + __ffs(b) - 1;
+                        break;
+                    }
+                }
+                const bool end = stop < 0 && start + 32 * c >= r1;
+                if (lane == 0) {
+                    scanned += min(r1, stop >= 0 ? stop + 1 : start + 32 * c) - start;
+                    if (stop >= 0)
+                        a.pos[v] = stop;
+                    else if (end)
+                        state[v] = kIn;
+                    else {
+                        a.pos[v] = start + 32 * kMisWarpChunks - 1;
+                        a.longq2[atomicAdd(l2len, 1)] = v;
+                    }
+                }
+                wq.push(stop >= 0 && lane == 0, v);
+                wj.push(end && lane == 0, v);
+            }
+            wq.flush();
+            wj.flush();
+            if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 4)) return;
+        }
+
+        // phase L2: the longest scans, one block per vertex
+        const int n2 = n1 > 0 ? ld_volatile_i32(l2len) : 0;
+        if (n2 > 0) {
+            for (int k = blockIdx.x; k < n2; k += G) {
+                const int v = __ldcg(a.longq2 + k);
+                const int r1 = __ldg(a.row_ptr + v + 1);
+                const int start = __ldcg(a.pos + v) + 1;
+                const unsigned pv = __ldg(a.prio + v);
                 if (threadIdx.x == 0) s_stop = kInf;
                 __syncthreads();
                 for (int b0 = start; b0 < r1; b0 += kBlock) {
                     const int idx = b0 + threadIdx.x;
-                    bool st = false;
-                    if (idx < r1) {
-                        const int u = __ldg(col + idx);
-                        const unsigned pu = __ldg(prio + u);
-                        const unsigned char su = __ldcg(state + u);
-                        st = u != v && su != kOut && outranks(pu, u, pv, v);
-                    }
+                    const bool st = idx < r1 && mis_stop(a, idx, v, pv);
                     if (st) atomicMin(&s_stop, idx);
                     if (__syncthreads_or(st)) break;
                 }
@@ -1039,14 +1056,15 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                         qn[atomicAdd(qlen_next, 1)] = v;
                     } else {
                         state[v] = kIn;
-                        qn[atomicAdd(qlen_next, 1)] = v | kJoinEntry;
+                        a.joined[atomicAdd(jlen_next, 1)] = v;
                     }
                 }
                 __syncthreads();
             }
-            if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 4)) return;
+            if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 5)) return;
         }
         cur ^= 1;
+        jc ^= 1;
     }
     long long insz = 0;
     for (int i = gtid; i < m; i += gstride) {
@@ -1429,7 +1447,9 @@ static apspie_status mis_common(apspie_ctx *ctx, const apspie_csr *A, const uint
     a.member_i32 = d_member_i32;
     a.buf = carve_trav(base, A->m);
     a.pos = a.buf.aux;
+    a.joined = a.buf.q3;
     a.longq = a.buf.q2;
+    a.longq2 = a.buf.aux2;
     Carver c(static_cast<char *>(base) + tb);
     a.state = c.take<unsigned char>(A->m);
     a.ctl = ctx->d_ctl;
