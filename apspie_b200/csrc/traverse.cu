@@ -787,9 +787,9 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_group_kernel(Ss
 // MIS
 // ================================================================================
 enum : unsigned char { kUndecided = 0, kIn = 1, kOut = 2 };
-constexpr int kMisGroup = 4;    // lanes that scan one vertex's row together (phase S)
-constexpr int kMisChunks = 4;   // chunks of kMisGroup neighbours a group scans before handing on
-constexpr int kMisWarpChunks = 64;  // chunks of 32 neighbours a warp scans (phase L) before handing on
+constexpr int kMisThread = 16;     // neighbours one thread scans (phase S) before handing the vertex on
+constexpr int kMisWarpChunks = 8;  // chunks of 32 neighbours a warp scans (phase L) before handing on
+constexpr int kMisLightRow = 64;   // joined vertices with at most this many neighbours push by one thread
 
 struct MisArgs {
     int m, nnz;
@@ -835,13 +835,14 @@ __device__ __forceinline__ bool mis_stop(const MisArgs &a, int idx, int v, unsig
 // once over the whole run and mostly not to their end (about 6.8M of R-MAT scale 20's
 // 31.4M entries). Vertices without neighbours join at the start. Round r, over the queue
 // of undecided vertices and the list of vertices that joined in round r-1:
-//  phase A  row lengths of the joined vertices (merge-path scan);
-//  phase P  they write out into their neighbours (merge-path expansion);
-//  phase S  each undecided vertex, by a group of kMisGroup lanes: out -> leaves; its
-//           blocker still undecided (or in: its push comes next round) -> waits; else it
-//           scans on in chunks of kMisGroup and stops at the first neighbour that outranks
-//           it and is not out (its new blocker); no such neighbour -> it joins. After
-//           kMisChunks chunks without an end the vertex goes to the long list;
+//  phase A  row lengths of the joined vertices with more than kMisLightRow neighbours;
+//  phase P  the joined vertices write out into their neighbours: short rows one thread
+//           each, long rows through the merge-path expansion;
+//  phase S  each undecided vertex, by one thread: out -> leaves; its blocker still
+//           undecided (or in: its push comes next round) -> waits; else it scans on, four
+//           neighbours a step, and stops at the first neighbour that outranks it and is not
+//           out (its new blocker); no such neighbour -> it joins. After kMisThread
+//           neighbours without an end the vertex goes to the long list;
 //  phase L  (only when that list is not empty) one warp per vertex goes on in chunks of
 //           32, for up to kMisWarpChunks chunks; the rest (phase L2) one block each.
 // The pushes of a round are complete before its scans start, so a scan sees every
@@ -887,9 +888,6 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
     int cur = 0, jc = 0;
     long long expanded = 0, scanned = 0;
     int round = 0;
-    const int gl = lane / kMisGroup, ll = lane % kMisGroup;
-    const unsigned gmask = ((1u << kMisGroup) - 1u) << (gl * kMisGroup);
-    constexpr int kGroupsPerWarp = 32 / kMisGroup;
     for (;;) {
         const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
         const int nj = ld_volatile_i32(jlen + jc);
@@ -904,9 +902,9 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         int *qlen_next = &a.ctl->qlen[cur ^ 1];
         int *jlen_next = jlen + (jc ^ 1);
 
-        // phase A: row lengths of the joined vertices
+        // phase A: row lengths of the joined vertices with long rows
         frontier_phase_a<kBlock>(a.joined, nj, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum, sm.scan_tmp,
-                                 [](int, int, int deg) { return deg; });
+                                 [](int, int, int deg) { return deg > kMisLightRow ? deg : 0; });
         if (gtid == 0) {
             *qlen_next = 0;
             *jlen_next = 0;
@@ -915,84 +913,100 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         }
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 1)) return;
 
-        // phase P: knock-outs
+        // phase P: knock-outs -- short rows by one thread each, long rows by the expansion
         const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
-        if (E > 0) {
+        if (nj > 0) {
             expanded += E;
-            const int *jl = a.joined;
-            frontier_expand<kBlock, kVT, true, false>(
-                nj, E, a.buf.loc_off, a.buf.rs, sm, [&](int j, int k, WarpSlice &ws) { ws.aux[k] = __ldcg(jl + j); },
-                [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT], WarpSlice &ws) {
-                    int u[kVT];
+            for (int i = gtid; i < nj; i += gstride) {
+                const int j = __ldcg(a.joined + i);
+                const int r0 = __ldg(a.row_ptr + j), r1 = __ldg(a.row_ptr + j + 1);
+                if (r1 - r0 > kMisLightRow) continue;
+                expanded += r1 - r0;
+                for (int e = r0; e < r1; e += 4) {
+                    int u[4];
 #pragma unroll
-                    for (int r = 0; r < kVT; ++r) u[r] = valid[r] ? __ldg(col + idx[r]) : 0;
+                    for (int k = 0; k < 4; ++k) u[k] = e + k < r1 ? __ldg(col + e + k) : j;
 #pragma unroll
-                    for (int r = 0; r < kVT; ++r)
-                        if (valid[r] && u[r] != ws.aux[kk[r]]) state[u[r]] = kOut;  // never in the set
-                },
-                NoPost());
+                    for (int k = 0; k < 4; ++k)
+                        if (u[k] != j) state[u[k]] = kOut;  // never in the set
+                }
+            }
+            if (E > 0) {
+                const int *jl = a.joined;
+                frontier_expand<kBlock, kVT, true, false>(
+                    nj, E, a.buf.loc_off, a.buf.rs, sm, [&](int jj, int k, WarpSlice &ws) { ws.aux[k] = __ldcg(jl + jj); },
+                    [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT], WarpSlice &ws) {
+                        int u[kVT];
+#pragma unroll
+                        for (int r = 0; r < kVT; ++r) u[r] = valid[r] ? __ldg(col + idx[r]) : 0;
+#pragma unroll
+                        for (int r = 0; r < kVT; ++r)
+                            if (valid[r] && u[r] != ws.aux[kk[r]]) state[u[r]] = kOut;
+                    },
+                    NoPost());
+            }
             if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 2)) return;
         }
 
-        // phase S: blocker checks, short scans and decisions, kGroupsPerWarp vertices a warp
+        // phase S: blocker checks, short scans and decisions, one thread per vertex; each
+        // step loads four neighbours at once and takes the first that decides anything
         {
             WQ wq(sm.qbuf[wid][0], qn, qlen_next);
             WQ wj(sm.qbuf[wid][1], a.joined, jlen_next);
-            const int gw = gtid >> 5, nw = gstride >> 5;
-            for (int wb = gw * kGroupsPerWarp; wb < nf; wb += nw * kGroupsPerWarp) {
-                const int i = wb + gl;
-                const int v = i < nf ? __ldcg(qc + i) : 0;
-                bool scanning = false, keep = false, joined = false, handed = false;
-                int start = 0, r1 = 0;
-                unsigned pv = 0;
-                if (i < nf && __ldcg(state + v) == kUndecided) {
-                    const int r0 = __ldg(a.row_ptr + v);
-                    r1 = __ldg(a.row_ptr + v + 1);
-                    const int p = __ldcg(a.pos + v);
-                    scanning = p < r0 || __ldcg(state + __ldg(col + p)) == kOut;
-                    keep = !scanning;  // its blocker is undecided, or joined (and pushes next round)
-                    start = p + 1;
-                    pv = __ldg(a.prio + v);
-                }
-                int stop = -1;
-                bool done = !scanning;
+            for (int base = blockIdx.x * kBlock; base < nf; base += gstride) {
+                const int i = base + threadIdx.x;
+                bool keep = false, joined = false;
+                int v = 0;
+                if (i < nf) {
+                    v = __ldcg(qc + i);
+                    if (__ldcg(state + v) == kUndecided) {
+                        const int r0 = __ldg(a.row_ptr + v), r1 = __ldg(a.row_ptr + v + 1);
+                        const int p = __ldcg(a.pos + v);
+                        if (p >= r0 && __ldcg(state + __ldg(col + p)) != kOut) {
+                            keep = true;  // its blocker is undecided, or joined (and pushes next round)
+                        } else {
+                            const unsigned pv = __ldg(a.prio + v);
+                            const int start = p + 1, lim = min(r1, start + kMisThread);
+                            int stop = -1, e = start;
+                            for (; e < lim && stop < 0; e += 4) {
+                                int u[4];
+                                unsigned pu[4];
+                                unsigned char su[4];
 #pragma unroll
-                for (int c = 0; c < kMisChunks; ++c) {
-                    const int idx = start + c * kMisGroup + ll;
-                    const bool st = !done && idx < r1 && mis_stop(a, idx, v, pv);
-                    const unsigned b = __ballot_sync(0xffffffffu, st) & gmask;
-                    if (!done) {
-                        if (b) {
-                            stop = start + c * kMisGroup + (__ffs(b) - 1 - gl * kMisGroup);
-                            done = true;
-                        } else if (start + (c + 1) * kMisGroup >= r1) {
-                            joined = true;
-                            done = true;
+                                for (int k = 0; k < 4; ++k) u[k] = e + k < lim ? __ldg(col + e + k) : v;
+#pragma unroll
+                                for (int k = 0; k < 4; ++k) {
+                                    pu[k] = __ldg(a.prio + u[k]);
+                                    su[k] = __ldcg(state + u[k]);
+                                }
+#pragma unroll
+                                for (int k = 0; k < 4; ++k)
+                                    if (stop < 0 && u[k] != v && su[k] != kOut && outranks(pu[k], u[k], pv, v))
+                                        stop = e + k;
+                            }
+                            scanned += (stop >= 0 ? stop + 1 : lim) - start;
+                            if (stop >= 0) {
+                                keep = true;
+                                a.pos[v] = stop;
+                            } else if (lim >= r1) {
+                                joined = true;
+                                state[v] = kIn;
+                            } else {  // settled up to lim - 1: a warp goes on
+                                a.pos[v] = lim - 1;
+                                a.longq[atomicAdd(l1len, 1)] = v;
+                            }
                         }
                     }
                 }
-                if (scanning) {
-                    if (ll == 0) scanned += min(r1, stop >= 0 ? stop + 1 : start + kMisChunks * kMisGroup) - start;
-                    if (stop >= 0) {
-                        keep = true;
-                        if (ll == 0) a.pos[v] = stop;
-                    } else if (joined) {
-                        if (ll == 0) state[v] = kIn;
-                    } else {
-                        handed = true;  // settled up to start + kMisChunks * kMisGroup - 1
-                        if (ll == 0) a.pos[v] = start + kMisChunks * kMisGroup - 1;
-                    }
-                }
-                wq.push(keep && ll == 0, v);
-                wj.push(joined && ll == 0, v);
-                if (handed && ll == 0) a.longq[atomicAdd(l1len, 1)] = v;
+                wq.push(keep, v);
+                wj.push(joined, v);
             }
             wq.flush();
             wj.flush();
         }
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 3)) return;
 
-        // phase L: longer scans, one warp per vertex
+        // phase L: longer scans, one warp per vertex (up to kMisWarpChunks chunks of 32)
         const int n1 = ld_volatile_i32(l1len);
         if (n1 > 0) {
             WQ wq(sm.qbuf[wid][0], qn, qlen_next);

@@ -613,7 +613,7 @@ def extras_batched(ctx, args, ws, local, g):
 SERVE_QUERIES = 100_000  # the serving stream's full length
 SERVE_SLOTS = 2
 SERVE_MAX_BATCH = 512
-POOL_ROWS = 512  # output rows per graph a stream keeps in flight (int32 rows; MIS: 64)
+POOL_ROWS = 1536  # output rows per graph a stream keeps in flight (int32 rows; MIS: 64)
 
 
 class RowHasher:
