@@ -87,7 +87,7 @@ class TuneParams(ctypes.Structure):
 class ServerStats(ctypes.Structure):
     _fields_ = [(n, c_int64) for n in ("submitted", "completed", "failed", "launches", "batched_queries",
                                         "max_batch_seen", "deferred", "peak_bytes", "resident_bytes",
-                                        "joined_running", "trivial")]
+                                        "joined_running", "trivial", "engine_launches", "engine_levels")]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

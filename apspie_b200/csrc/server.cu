@@ -387,7 +387,10 @@ void engine_ended(apspie_server *s, Slot &sl, std::map<std::pair<int, int>, std:
     const int gi = sl.engine_graph;
     Graph &g = s->graphs[gi];
     engine_completions(s, g);
-    const apspie_status st = slot_device_status(sl);
+    apspie_run_stats rs;
+    // the control block back (levels run) and the launch's device status
+    apspie_status st = finish_call(sl.ctx, &rs, "bfs engine");
+    if (st == APSPIE_OK) st = slot_device_status(sl);
     std::vector<Request> back;
     for (unsigned long long id : bfs_engine_take_back(g.eng)) {
         auto it = g.in_engine.find(id);
@@ -414,6 +417,8 @@ void engine_ended(apspie_server *s, Slot &sl, std::map<std::pair<int, int>, std:
     {
         std::lock_guard<std::mutex> lock(s->mu);
         s->st.launches += 1;
+        s->st.engine_launches += 1;
+        s->st.engine_levels += rs.iterations;
         if (fail) {
             const auto now = Clock::now();
             for (const Request &r : back) complete_locked(s, r, st, now);

@@ -812,12 +812,19 @@ __device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v)
     return pu > pv || (pu == pv && u > v);
 }
 
+// A neighbour's state as a scan reads it: through L1, so the hot lines of high-degree
+// neighbours (read by many scans at once) are not all fetched from L2. A stale value is
+// safe here: states only move from undecided to in or out, so a stale read can only make
+// a scan stop early at a neighbour that is already out, and the next round's blocker check
+// (a coherent read) sees it out and resumes the scan behind it.
+__device__ __forceinline__ unsigned char scan_state(const unsigned char *state, int u) { return state[u]; }
+
 // One neighbour of a scanning vertex v: does it decide anything (an outranking neighbour
 // that is not out: v's new blocker, or -- if in -- the vertex whose push knocks v out)?
 __device__ __forceinline__ bool mis_stop(const MisArgs &a, int idx, int v, unsigned pv) {
     const int u = __ldg(a.col_ind + idx);
     const unsigned pu = __ldg(a.prio + u);
-    const unsigned char su = __ldcg(a.state + u);
+    const unsigned char su = scan_state(a.state, u);
     return u != v && su != kOut && outranks(pu, u, pv, v);
 }
 
@@ -927,8 +934,8 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
 #pragma unroll
                     for (int k = 0; k < 4; ++k) u[k] = e + k < r1 ? __ldg(col + e + k) : j;
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        if (u[k] != j) state[u[k]] = kOut;  // never in the set
+                    for (int k = 0; k < 4; ++k)  // never in the set; many joiners share hubs: skip known outs
+                        if (u[k] != j && scan_state(state, u[k]) != kOut) state[u[k]] = kOut;
                 }
             }
             if (E > 0) {
@@ -941,7 +948,8 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                         for (int r = 0; r < kVT; ++r) u[r] = valid[r] ? __ldg(col + idx[r]) : 0;
 #pragma unroll
                         for (int r = 0; r < kVT; ++r)
-                            if (valid[r] && u[r] != ws.aux[kk[r]]) state[u[r]] = kOut;
+                            if (valid[r] && u[r] != ws.aux[kk[r]] && scan_state(state, u[r]) != kOut)
+                                state[u[r]] = kOut;
                     },
                     NoPost());
             }
@@ -977,7 +985,8 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
 #pragma unroll
                                 for (int k = 0; k < 4; ++k) {
                                     pu[k] = __ldg(a.prio + u[k]);
-                                    su[k] = __ldcg(state + u[k]);
+                                    // in the first round every vertex with neighbours is undecided
+                                    su[k] = round == 1 ? kUndecided : scan_state(state, u[k]);
                                 }
 #pragma unroll
                                 for (int k = 0; k < 4; ++k)

@@ -842,6 +842,7 @@ def extras_serving(ctx, args, local, g22):
         "queries": n, "plain_qps": plain_qps, "server_qps": n / tot_s, "x_plain": tot_p / tot_s,
         "saturated": {"server": _pct(lat_s), "plain": _pct(lat_p)},
         "launches": st["launches"], "joined_running": st["joined_running"], "trivial": st["trivial"],
+        "engine_launches": st["engine_launches"], "engine_levels": st["engine_levels"],
         "max_batch_seen": st["max_batch_seen"], "peak_bytes": st["peak_bytes"],
         "exact_checked": n, "exact_equal": same, "exact": same == n}}
     for mult in (0.8, 2.0):
@@ -870,6 +871,7 @@ def extras_serving(ctx, args, local, g22):
         "queries": n, "plain_qps": n / tot_p, "server_qps": n / tot_s, "x_plain": tot_p / tot_s,
         "server": _pct(lat_s), "plain": _pct(lat_p), "launches": st["launches"],
         "joined_running": st["joined_running"], "trivial": st["trivial"], "max_batch_seen": st["max_batch_seen"],
+        "engine_launches": st["engine_launches"], "engine_levels": st["engine_levels"],
         "exact_checked": n, "exact": same == n}
     return res
 

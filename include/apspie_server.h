@@ -43,6 +43,8 @@ typedef struct apspie_server_stats {
     int64_t resident_bytes;   /* graphs + per-slot reserved scratch */
     int64_t joined_running;   /* BFS requests posted into an engine launch already on the GPU */
     int64_t trivial;          /* BFS / SSSP requests whose source has no edges (no traversal) */
+    int64_t engine_launches;  /* BFS engine launches (each runs until nothing is in flight or waiting) */
+    int64_t engine_levels;    /* BFS levels those launches ran, summed */
 } apspie_server_stats;
 
 /* device: GPU ordinal; memory_budget_bytes: device bytes the server may hold (graphs,

@@ -9,8 +9,8 @@ neighbours (phase P, complete before the scans start); then every undecided vert
 steps interleaved at random with every other vertex's steps: leaves if it is out, waits if
 its blocker is still undecided (or in), else scans the rest of its row in chunks of 1-3
 neighbours, stopping at the first that outranks it and is not out, and then decides at
-once -- joining (state in, read by the others' later steps) when it found no stop. No GPU
-is involved."""
+once -- joining (state in, read by the others' later steps) when it found no stop. Scans may
+read stale states (as through L1); blocker checks read current ones. No GPU is involved."""
 import numpy as np
 import pytest
 
@@ -34,9 +34,11 @@ def _run_model(rp, ci, prio, rng, mistake=None):
             queue.append((v, False))
         else:
             state[v] = IN
-    for _ in range(n + 3):
+    snaps = [state.copy()]  # states at the start of earlier rounds (what an L1 may still hold)
+    for _ in range(4 * n + 8):
         if not queue:
             return state
+        snaps = (snaps + [state.copy()])[-3:]
         # phase P
         for v, joined in queue:
             if joined:
@@ -60,7 +62,10 @@ def _run_model(rp, ci, prio, rng, mistake=None):
                 k = int(rng.integers(1, 4))
                 for x in range(e, min(e + k, r1)):
                     u = int(ci[x])
-                    if u != v and state[u] != OUT and _outranks(prio[u], u, prio[v], v):
+                    # scans may read a stale state (through L1): the current one or one from
+                    # the start of this or an earlier round
+                    su = state[u] if rng.random() < 0.5 else snaps[int(rng.integers(0, len(snaps)))][u]
+                    if u != v and su != OUT and _outranks(prio[u], u, prio[v], v):
                         stop = x
                         break
                 e += k
