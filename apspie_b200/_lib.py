@@ -158,8 +158,10 @@ SIGNATURES = {
     "apspie_server_set_sssp_fold": (c_int, [c_void_p, c_int32]),
     "apspie_server_set_bfs_min_batch": (c_int, [c_void_p, c_int32]),
     "apspie_server_set_sssp_min_batch": (c_int, [c_void_p, c_int32]),
+    "apspie_server_set_side_room": (c_int, [c_void_p, c_int32]),
     "apspie_server_start": (c_int, [c_void_p]),
     "apspie_server_submit": (c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, POINTER(ctypes.c_uint64)]),
+    "apspie_server_submit_many": (c_int, [c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "apspie_server_wait": (c_int, [c_void_p, ctypes.c_uint64, c_int32, POINTER(c_double)]),
     "apspie_server_take_completed": (c_int, [c_void_p, c_int32, c_int32, c_void_p, c_void_p, c_void_p,
                                              POINTER(c_int32)]),

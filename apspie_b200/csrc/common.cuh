@@ -44,6 +44,10 @@ struct TravCtl {
     // queue and a degree-weighted histogram of its distances. Device-only.
     int sbase[2];
     unsigned long long shist[2][kBandBins];
+    // Per-round list counters of kernels that keep several rounds' lists apart (MIS keeps
+    // three: the lists a round fills, reads, and clears for the round after next). Device-only.
+    int rcnt[12];
+    unsigned long long rcnt64[3];
 };
 static_assert(offsetof(TravCtl, bar) == 0 && offsetof(TravCtl, err) == 4, "barrier word / error pair");
 // Prefix of the control block the host reads back after a call.
@@ -99,6 +103,7 @@ struct apspie_ctx {
     long long sssp_band = 0;  // 0: auto, < 0: off
     int max_grid = 0;    // 0: as many co-resident blocks as fit
     int grid_share = 1;  // persistent grids take 1/grid_share of the co-resident capacity
+    int side_room = 0;   // persistent grids with the device to themselves leave kSideRoomRegs per SM
     float batch_push_frac = 0.05f;  // batched BFS: push while frontier edges < frac * nnz
     int spgemm_reg_max = 128;       // SpGEMM register tier: rows of <= this many products
     int spgemm_block_max = 1024;    // SpGEMM shared-table tier: rows of <= this many products
@@ -129,7 +134,13 @@ apspie_status validate_csr(apspie_ctx *ctx, const apspie_csr *A, bool need_squar
 // Checks host-visible CSR view fields (no device access).
 apspie_status check_csr_view(apspie_ctx *ctx, const apspie_csr *A, const char *who);
 // Co-resident blocks a persistent kernel with per_sm blocks per SM may launch on ctx.
-int persistent_cap(const apspie_ctx *ctx, int per_sm);
+// With ctx->side_room and the device to itself (grid_share 1), it takes fewer blocks per
+// SM until kSideRoomRegs registers per SM stay free (regs_per_block: the kernel's register
+// allocation per block), so that small kernels of other streams (the server's answers for
+// sources without edges, a caller's own kernels) still find room on every SM.
+constexpr int kSmRegs = 65536;        // registers per SM (sm_100a)
+constexpr int kSideRoomRegs = 4096;   // e.g. two 64-thread blocks of up to 32 registers
+int persistent_cap(const apspie_ctx *ctx, int per_sm, int regs_per_block = 0);
 // Cooperative launch of a persistent kernel with the largest co-resident grid.
 // `work` (edges the graph holds) sizes the grid: about one block per kWorkPerBlock edges,
 // at least one per SM, at most the co-resident limit (barrier cost grows with blocks).

@@ -150,12 +150,14 @@ __global__ void barrier_check_kernel(TravCtl *ctl, int *sticky, int rounds, int 
         if (!grid_barrier(ctl, sticky, 900 + r)) return;
 }
 
-int persistent_cap(const apspie_ctx *ctx, int per_sm) {
+int persistent_cap(const apspie_ctx *ctx, int per_sm, int regs_per_block) {
     // a context that shares the device with grid_share - 1 others takes 1/grid_share of the
     // co-resident capacity, so that all of them fit at once. Whole blocks per SM: then each
     // kernel holds at most 1/grid_share of every per-SM resource (registers, shared memory,
     // threads), whichever limits it, and kernels of different footprints still fit together
     const int share = std::max(1, ctx->grid_share);
+    if (share == 1 && ctx->side_room && regs_per_block > 0)
+        while (per_sm > 1 && per_sm * regs_per_block > kSmRegs - kSideRoomRegs) --per_sm;
     if (per_sm >= share) return per_sm / share * ctx->num_sms;
     return std::max(1, per_sm * ctx->num_sms / share);
 }
@@ -166,7 +168,14 @@ apspie_status launch_persistent(apspie_ctx *ctx, const void *func, int block, vo
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, block, 0);
     if (e != cudaSuccess) return cuda_error(ctx, e, "occupancy query");
     if (per_sm < 1) return set_error(ctx, APSPIE_ERR_CUDA, "persistent kernel cannot be resident");
-    const int cap = persistent_cap(ctx, per_sm);
+    int regs_per_block = 0;
+    if (ctx->side_room) {
+        cudaFuncAttributes fa;
+        if ((e = cudaFuncGetAttributes(&fa, func)) != cudaSuccess) return cuda_error(ctx, e, "kernel attributes");
+        // registers are allocated per warp in units of 256
+        regs_per_block = (fa.numRegs * 32 + 255) / 256 * 256 * ((block + 31) / 32);
+    }
+    const int cap = persistent_cap(ctx, per_sm, regs_per_block);
     int grid = cap;
     const long long want = (work + kWorkPerBlock - 1) / kWorkPerBlock;
     if (want < grid) grid = static_cast<int>(want < ctx->num_sms ? ctx->num_sms : want);

@@ -112,10 +112,31 @@ struct TrivialArgs {
     int *row[kTrivialMax];
 };
 
+// Every entry -1 but the source's 0. Rows whose start is 16-byte aligned are written four
+// entries per store.
 __global__ void trivial_rows(TrivialArgs t) {
-    for (int k = 0; k < t.n; ++k)
-        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < t.m; i += gridDim.x * blockDim.x)
-            t.row[k][i] = i == t.src[k] ? 0 : -1;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    for (int k = 0; k < t.n; ++k) {
+        int *row = t.row[k];
+        const int src = t.src[k];
+        int done = 0;
+        if ((reinterpret_cast<uintptr_t>(row) & 15u) == 0) {
+            const int n4 = t.m >> 2;
+            for (int i = tid; i < n4; i += stride) {
+                int4 x = make_int4(-1, -1, -1, -1);
+                if (i == src >> 2) {
+                    const int lane = src & 3;
+                    x.x = lane == 0 ? 0 : -1;
+                    x.y = lane == 1 ? 0 : -1;
+                    x.z = lane == 2 ? 0 : -1;
+                    x.w = lane == 3 ? 0 : -1;
+                }
+                reinterpret_cast<int4 *>(row)[i] = x;
+            }
+            done = n4 << 2;
+        }
+        for (int i = done + tid; i < t.m; i += stride) row[i] = i == src ? 0 : -1;
+    }
 }
 
 struct TrivialLaunch {
@@ -349,8 +370,9 @@ void launch_trivial(apspie_server *s, std::vector<Request> &reqs) {
             tl.reqs.push_back(reqs[i]);
             ++i;
         }
-        const int blocks = std::min(1024, (t.m + 255) / 256);
-        trivial_rows<<<blocks, 256, 0, s->triv_stream>>>(t);
+        // 64-thread blocks: they fit beside a persistent grid (see side_room)
+        const int blocks = std::min(2048, (t.m + 63) / 64);
+        trivial_rows<<<blocks, 64, 0, s->triv_stream>>>(t);
         if (s->free_events.empty()) {
             cudaEvent_t ev;
             cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
@@ -650,6 +672,9 @@ apspie_status apspie_server_create(int device, int64_t memory_budget_bytes, int3
         // then retried on half the grid.)
         sl.share = num_slots;
         sl.ctx->grid_share = num_slots;
+        // a slot's grid that has the device to itself still leaves room for the answers of
+        // sources without edges (a kernel on the side stream) and the caller's kernels
+        sl.ctx->side_room = 1;
     }
     *out = s;
     return APSPIE_OK;
@@ -717,6 +742,12 @@ apspie_status apspie_server_set_sssp_min_batch(apspie_server *s, int32_t min_bat
     return APSPIE_OK;
 }
 
+apspie_status apspie_server_set_side_room(apspie_server *s, int32_t on) {
+    if (!s || s->started) return APSPIE_ERR_INVALID_ARG;
+    for (auto &sl : s->slots) sl.ctx->side_room = on != 0;
+    return APSPIE_OK;
+}
+
 apspie_status apspie_server_start(apspie_server *s) {
     if (!s || s->started) return APSPIE_ERR_INVALID_ARG;
     // reserve each slot's scratch up front so admission accounting matches the device: the
@@ -749,27 +780,42 @@ apspie_status apspie_server_start(apspie_server *s) {
 
 apspie_status apspie_server_submit(apspie_server *s, int32_t graph_id, int32_t kind, int32_t source, void *d_out,
                                    uint64_t *ticket) {
-    if (!s || !ticket || !d_out || !s->started) return APSPIE_ERR_INVALID_ARG;
-    if (graph_id < 0 || graph_id >= static_cast<int32_t>(s->graphs.size())) return APSPIE_ERR_INVALID_ARG;
-    if (kind != APSPIE_QUERY_BFS && kind != APSPIE_QUERY_SSSP && kind != APSPIE_QUERY_MIS) return APSPIE_ERR_INVALID_ARG;
-    const Graph &g = s->graphs[graph_id];
-    if (kind != APSPIE_QUERY_MIS && (source < 0 || source >= g.view.m)) return APSPIE_ERR_INVALID_ARG;
-    if (kind == APSPIE_QUERY_SSSP && g.view.val_type != APSPIE_VAL_I32) return APSPIE_ERR_UNSUPPORTED;
-    Request r;
-    r.graph = graph_id;
-    r.kind = kind;
-    r.source = kind == APSPIE_QUERY_MIS ? 0 : source;
-    r.d_out = d_out;
-    r.t_submit = Clock::now();
+    if (!ticket) return APSPIE_ERR_INVALID_ARG;
+    return apspie_server_submit_many(s, 1, &graph_id, &kind, &source, &d_out, ticket);
+}
+
+apspie_status apspie_server_submit_many(apspie_server *s, int32_t n, const int32_t *graph_ids, const int32_t *kinds,
+                                        const int32_t *sources, void *const *d_outs, uint64_t *tickets) {
+    if (!s || n < 0 || !s->started) return APSPIE_ERR_INVALID_ARG;
+    if (n == 0) return APSPIE_OK;
+    if (!graph_ids || !kinds || !sources || !d_outs || !tickets) return APSPIE_ERR_INVALID_ARG;
+    for (int32_t i = 0; i < n; ++i) {
+        const int32_t gi = graph_ids[i], kind = kinds[i];
+        if (!d_outs[i] || gi < 0 || gi >= static_cast<int32_t>(s->graphs.size())) return APSPIE_ERR_INVALID_ARG;
+        if (kind != APSPIE_QUERY_BFS && kind != APSPIE_QUERY_SSSP && kind != APSPIE_QUERY_MIS)
+            return APSPIE_ERR_INVALID_ARG;
+        const Graph &g = s->graphs[gi];
+        if (kind != APSPIE_QUERY_MIS && (sources[i] < 0 || sources[i] >= g.view.m)) return APSPIE_ERR_INVALID_ARG;
+        if (kind == APSPIE_QUERY_SSSP && g.view.val_type != APSPIE_VAL_I32) return APSPIE_ERR_UNSUPPORTED;
+    }
+    const auto now = Clock::now();
     {
         std::lock_guard<std::mutex> lock(s->mu);
-        r.ticket = s->next_ticket++;
-        s->results[r.ticket] = Done();
-        s->incoming.push_back(r);
-        s->st.submitted += 1;
+        for (int32_t i = 0; i < n; ++i) {
+            Request r;
+            r.graph = graph_ids[i];
+            r.kind = kinds[i];
+            r.source = kinds[i] == APSPIE_QUERY_MIS ? 0 : sources[i];
+            r.d_out = d_outs[i];
+            r.t_submit = now;
+            r.ticket = s->next_ticket++;
+            s->results[r.ticket] = Done();
+            s->incoming.push_back(r);
+            tickets[i] = r.ticket;
+        }
+        s->st.submitted += n;
     }
     s->cv_work.notify_one();
-    *ticket = r.ticket;
     return APSPIE_OK;
 }
 

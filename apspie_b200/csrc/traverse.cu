@@ -34,15 +34,13 @@ namespace {
 
 constexpr int kBlock = 256;
 constexpr int kVT = 4;
-using Smem = ExpandSmem<kBlock, kVT>;          // MIS (uses the extra per-entry arrays)
-using WarpSlice = Smem::Warp;
 using BfsSmem = ExpandSmem<kBlock, kVT, false>;
 using BfsSlice = BfsSmem::Warp;
 constexpr int kSsspVT = APSPIE_SSSP_VT;
 constexpr int kSsspPA = 4;  // frontier entries per thread per phase-A step
 using SsspSmem = ExpandSmem<kBlock, kSsspVT, false>;
 using SsspSlice = SsspSmem::Warp;
-using WQ = WarpQueue<Smem::QCAP>;
+using WQ = WarpQueue<BfsSmem::QCAP>;
 
 struct NoPost {
     template <class S>
@@ -789,7 +787,7 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_group_kernel(Ss
 enum : unsigned char { kUndecided = 0, kIn = 1, kOut = 2 };
 constexpr int kMisThread = 16;     // neighbours one thread scans (phase S) before handing the vertex on
 constexpr int kMisWarpChunks = 8;  // chunks of 32 neighbours a warp scans (phase L) before handing on
-constexpr int kMisLightRow = 64;   // joined vertices with at most this many neighbours push by one thread
+constexpr int kMisLightRow = 64;   // joiners with at most this many neighbours push by one thread
 
 struct MisArgs {
     int m, nnz;
@@ -799,11 +797,16 @@ struct MisArgs {
     unsigned char *member;
     int *member_i32;  // when set, the set is written here as int32 1/0 instead
     unsigned char *state;
-    int *pos;     // CSR index of the outranking neighbour that blocks the vertex (row start - 1: none yet)
-    int *joined;  // the vertices that joined in the last round (they push next round)
-    int *longq;   // scans that go on past a group's share this round (one warp each)
-    int *longq2;  // scans that go on past a warp's share (one block each)
-    TravBuffers buf;
+    int *pos;          // CSR index of the outranking neighbour that blocks the vertex (row start - 1: none yet)
+    int *queue[2];     // undecided vertices, by round parity
+    int *longq;        // scans that go on past a thread's share (one warp each, phase L)
+    int *longq2;       // scans that go on past a warp's share (one block each, phase L2)
+    int *light;        // vertices that joined with rows of at most kMisLightRow (pushed next round)
+    int *heavy_v;      // vertices that joined with longer rows,
+    int *heavy_base;   // the offset of each one's row in the next round's flat range of pushes,
+    int *heavy_delta;  // and row start - offset (push t of the range is CSR entry t + delta)
+    int *unit_owner;   // the heavy entry holding the first push of each unit of the range
+    int unit_shift;    // units of 1 << unit_shift pushes (one warp each)
     TravCtl *ctl;
     int *sticky;
 };
@@ -812,20 +815,43 @@ __device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v)
     return pu > pv || (pu == pv && u > v);
 }
 
-// A neighbour's state as a scan reads it: through L1, so the hot lines of high-degree
+// A neighbour's state as a scan reads it: through L1, so the lines of high-degree
 // neighbours (read by many scans at once) are not all fetched from L2. A stale value is
-// safe here: states only move from undecided to in or out, so a stale read can only make
-// a scan stop early at a neighbour that is already out, and the next round's blocker check
-// (a coherent read) sees it out and resumes the scan behind it.
+// safe: states only move from undecided to in or out, so a stale read can only make a scan
+// stop early at a neighbour that is already out, and the next round's blocker check (a
+// coherent read) sees it out and resumes the scan behind it.
 __device__ __forceinline__ unsigned char scan_state(const unsigned char *state, int u) { return state[u]; }
 
 // One neighbour of a scanning vertex v: does it decide anything (an outranking neighbour
-// that is not out: v's new blocker, or -- if in -- the vertex whose push knocks v out)?
+// that is not out: v's new blocker, or -- if in -- the vertex that knocks v out)?
 __device__ __forceinline__ bool mis_stop(const MisArgs &a, int idx, int v, unsigned pv) {
     const int u = __ldg(a.col_ind + idx);
     const unsigned pu = __ldg(a.prio + u);
     const unsigned char su = scan_state(a.state, u);
     return u != v && su != kOut && outranks(pu, u, pv, v);
+}
+
+// Knock out neighbour u of a vertex that joined. Many joiners share their high-degree
+// neighbours, and stores from many SMs into one line queue up in L2, so (check) a neighbour
+// already seen out (through L1: a stale "undecided" only costs a redundant store) is
+// skipped. In the first push round nothing is out yet.
+__device__ __forceinline__ void mis_knock(const MisArgs &a, int u, bool check) {
+    if (!check || scan_state(a.state, u) != kOut) a.state[u] = kOut;
+}
+
+// v joined with a row [r0, r0 + deg) longer than kMisLightRow: list it for the next
+// round's pushes. One atomic on (entries << 32 | pushes) gives the entry index and the
+// row's offset in the flat range, so offsets ascend with the index; the units starting
+// inside the row record it.
+__device__ __forceinline__ void mis_list_heavy(const MisArgs &a, unsigned long long *heavy, int v, int r0, int deg) {
+    const unsigned long long old = atomicAdd(heavy, (1ull << 32) | static_cast<unsigned>(deg));
+    const int idx = static_cast<int>(old >> 32);
+    const int base = static_cast<int>(old & 0xffffffffull);
+    a.heavy_v[idx] = v;
+    a.heavy_base[idx] = base;
+    a.heavy_delta[idx] = r0 - base;
+    const int sh = a.unit_shift;
+    for (int c = ((base - 1) >> sh) + 1; (c << sh) < base + deg; ++c) a.unit_owner[c] = idx;
 }
 
 // Greedy MIS in descending (priority, id) order -- the set spmspvMis converges to
@@ -840,24 +866,33 @@ __device__ __forceinline__ bool mis_stop(const MisArgs &a, int idx, int v, unsig
 // it is settled, and the neighbour at it is its current blocker (undecided, outranking).
 // Each scan stops at the first neighbour that decides anything, so rows are read about
 // once over the whole run and mostly not to their end (about 6.8M of R-MAT scale 20's
-// 31.4M entries). Vertices without neighbours join at the start. Round r, over the queue
-// of undecided vertices and the list of vertices that joined in round r-1:
-//  phase A  row lengths of the joined vertices with more than kMisLightRow neighbours;
-//  phase P  the joined vertices write out into their neighbours: short rows one thread
-//           each, long rows through the merge-path expansion;
+// 31.4M entries). Round r, over the undecided vertices (round 0: all of them, which also
+// sets every state; vertices without neighbours join there) and the vertices that joined
+// in round r - 1:
+//  phase P  (when anything joined) the joiners write out into their neighbours: rows of at
+//           most kMisLightRow one thread each; longer rows, laid end to end in the order
+//           they were listed, in equal units of 1 << unit_shift entries, one warp each.
+//           Only stores (and L1 reads): on the B200 a phase in which many SMs both store
+//           into and read the lines of high-degree vertices' states runs several times
+//           slower, so the pushes are not made by the joining threads during the scans;
 //  phase S  each undecided vertex, by one thread: out -> leaves; its blocker still
 //           undecided (or in: its push comes next round) -> waits; else it scans on, four
 //           neighbours a step, and stops at the first neighbour that outranks it and is not
-//           out (its new blocker); no such neighbour -> it joins. After kMisThread
-//           neighbours without an end the vertex goes to the long list;
+//           out (its new blocker); no such neighbour -> it joins and is listed for the next
+//           round's pushes. After kMisThread neighbours without an end the vertex goes to
+//           the long list;
 //  phase L  (only when that list is not empty) one warp per vertex goes on in chunks of
 //           32, for up to kMisWarpChunks chunks; the rest (phase L2) one block each.
-// The pushes of a round are complete before its scans start, so a scan sees every
-// vertex knocked out so far; scans and joins of the same phase race only safely (a vertex
-// joins only if every outranking neighbour was seen not to be, and out is final). The set
-// is the greedy MIS whatever the timing.
+// The pushes of a round are complete before its scans start, so a scan sees every vertex
+// knocked out so far; scans and joins of the same phase race only safely (a vertex joins
+// only if every outranking neighbour was seen out, and out is final). The set is the
+// greedy MIS whatever the timing.
+//
+// The lists a round fills (long lists and joiners in slot r mod 3 of the control block's
+// round counters, the next queue in slot r + 1) are cleared by the round before: their
+// last readers finished a full round earlier, so no block can still be reading them.
 __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
-    __shared__ Smem sm;
+    __shared__ int qbuf[kBlock / 32][3][BfsSmem::QCAP];
     __shared__ int s_stop;
     timeline_mark(a.ctl, 0);
     const int G = gridDim.x;
@@ -868,110 +903,114 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
     const int m = a.m;
     const int *col = a.col_ind;
     unsigned char *state = a.state;
-    int *jlen = &a.ctl->flen[0];             // [2]: joined-list lengths, by round parity
-    int *l1len = reinterpret_cast<int *>(&a.ctl->aux[0]);
-    int *l2len = reinterpret_cast<int *>(&a.ctl->aux[1]);
-    {
-        WQ wq(sm.qbuf[wid][0], a.buf.q0, &a.ctl->qlen[0]);
-        for (int base = blockIdx.x * kBlock; base < m; base += gstride) {
-            const int v = base + threadIdx.x;
-            bool q = false;
-            if (v < m) {
-                const int r0 = __ldg(a.row_ptr + v);
-                q = __ldg(a.row_ptr + v + 1) > r0;
-                a.state[v] = q ? kUndecided : kIn;  // no neighbours: in the set from the start
-                a.pos[v] = r0 - 1;
-            }
-            wq.push(q, v);
-        }
-        wq.flush();
-    }
-    if (gtid == 0) {
-        a.ctl->qlen[1] = 0;
-        jlen[0] = jlen[1] = 0;
-    }
-    if (!grid_barrier(a.ctl, a.sticky, kSiteMis)) return;
-
-    int cur = 0, jc = 0;
-    long long expanded = 0, scanned = 0;
-    int round = 0;
-    for (;;) {
-        const int nf = ld_volatile_i32(&a.ctl->qlen[cur]);
-        const int nj = ld_volatile_i32(jlen + jc);
-        if (nf == 0 && nj == 0) break;
-        if (round > m + 1) {
+    int *qlen = a.ctl->rcnt;                   // [3] undecided-queue lengths
+    int *l1len = a.ctl->rcnt + 3;              // [3] long list (phase L)
+    int *l2len = a.ctl->rcnt + 6;              // [3] longest list (phase L2)
+    int *nlight = a.ctl->rcnt + 9;             // [3] light joiners
+    unsigned long long *heavy = a.ctl->rcnt64;  // [3] (entries << 32) | pushes of heavy joiners
+    long long pushed = 0, scanned = 0;
+    int r = 0;
+    for (;; ++r) {
+        const int s0 = r % 3, s1 = (r + 1) % 3, s2 = (r + 2) % 3;
+        const int sp = (r + 2) % 3;  // the joiner lists of round r - 1
+        const int nf = r == 0 ? m : ld_volatile_i32(qlen + s0);  // round 0: every vertex
+        const int nl = ld_volatile_i32(nlight + sp);
+        const unsigned long long hh = __ldcg(reinterpret_cast<const unsigned long long *>(heavy + sp));
+        const int nh = static_cast<int>(hh >> 32);
+        const int H = static_cast<int>(hh & 0xffffffffull);
+        const int sh = a.unit_shift;
+        const int nu = H > 0 ? ((H - 1) >> sh) + 1 : 0;
+        if (nf == 0 && nl == 0 && nu == 0) break;
+        if (r > m + 1) {
             if (gtid == 0) raise_error(a.ctl, a.sticky, APSPIE_ERR_NOT_CONVERGED, kSiteMisRoundCap);
             break;
         }
-        ++round;
-        int *qc = cur ? a.buf.q1 : a.buf.q0;
-        int *qn = cur ? a.buf.q0 : a.buf.q1;
-        int *qlen_next = &a.ctl->qlen[cur ^ 1];
-        int *jlen_next = jlen + (jc ^ 1);
+        const int *qc = a.queue[r & 1];
+        int *qn = a.queue[(r & 1) ^ 1];
 
-        // phase A: row lengths of the joined vertices with long rows
-        frontier_phase_a<kBlock>(a.joined, nj, a.row_ptr, a.buf.rs, a.buf.loc_off, a.buf.chunk_sum, sm.scan_tmp,
-                                 [](int, int, int deg) { return deg > kMisLightRow ? deg : 0; });
-        if (gtid == 0) {
-            *qlen_next = 0;
-            *jlen_next = 0;
-            *l1len = 0;
-            *l2len = 0;
-        }
-        if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 1)) return;
-
-        // phase P: knock-outs -- short rows by one thread each, long rows by the expansion
-        const int E = frontier_chunk_bases<kBlock>(a.buf.chunk_sum, sm.base, sm.scan_tmp);
-        if (nj > 0) {
-            expanded += E;
-            for (int i = gtid; i < nj; i += gstride) {
-                const int j = __ldcg(a.joined + i);
+        // phase P: the last round's joiners knock out their neighbours -- short rows one
+        // thread each, long rows laid end to end and shared out in equal units, one warp
+        // each. Plain byte stores: every neighbour of a vertex in the set is out.
+        if (nl > 0 || nu > 0) {
+            // skipping known outs pays when many joiners share neighbours; with few of them
+            // the read before each store only lengthens the chain
+            const bool check = r >= 2 && nl + nh >= 4096;
+            for (int i = gtid; i < nl; i += gstride) {
+                const int j = __ldcg(a.light + i);
                 const int r0 = __ldg(a.row_ptr + j), r1 = __ldg(a.row_ptr + j + 1);
-                if (r1 - r0 > kMisLightRow) continue;
-                expanded += r1 - r0;
-                for (int e = r0; e < r1; e += 4) {
-                    int u[4];
+                pushed += r1 - r0;
+                for (int e = r0; e < r1; e += 8) {
+                    int u[8];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) u[k] = e + k < r1 ? __ldg(col + e + k) : j;
+                    for (int k = 0; k < 8; ++k) u[k] = e + k < r1 ? __ldg(col + e + k) : j;
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)  // never in the set; many joiners share hubs: skip known outs
-                        if (u[k] != j && scan_state(state, u[k]) != kOut) state[u[k]] = kOut;
+                    for (int k = 0; k < 8; ++k)
+                        if (u[k] != j) mis_knock(a, u[k], check);
                 }
             }
-            if (E > 0) {
-                const int *jl = a.joined;
-                frontier_expand<kBlock, kVT, true, false>(
-                    nj, E, a.buf.loc_off, a.buf.rs, sm, [&](int jj, int k, WarpSlice &ws) { ws.aux[k] = __ldcg(jl + jj); },
-                    [&](const bool (&valid)[kVT], const int (&kk)[kVT], const int (&idx)[kVT], WarpSlice &ws) {
-                        int u[kVT];
+            const int gw = gtid >> 5, nw = gstride >> 5;
+            for (int c = gw; c < nu; c += nw) {
+                // a unit spans the end of one row and the start of the next where rows meet in it
+                const int t0 = c << sh, t1 = min(H, t0 + (1 << sh));
+                int i = __ldcg(a.unit_owner + c);
+                int hv = __ldcg(a.heavy_v + i), hd = __ldcg(a.heavy_delta + i);
+                int nb = i + 1 < nh ? __ldcg(a.heavy_base + i + 1) : INT_MAX;
+                if (lane == 0) pushed += t1 - t0;
+                for (int tb = t0; tb < t1; tb += 128) {
+                    int e[4], w[4];
 #pragma unroll
-                        for (int r = 0; r < kVT; ++r) u[r] = valid[r] ? __ldg(col + idx[r]) : 0;
+                    for (int q = 0; q < 4; ++q) {
+                        const int t = tb + 32 * q + lane;
+                        while (t < t1 && t >= nb) {
+                            ++i;
+                            hv = __ldcg(a.heavy_v + i);
+                            hd = __ldcg(a.heavy_delta + i);
+                            nb = i + 1 < nh ? __ldcg(a.heavy_base + i + 1) : INT_MAX;
+                        }
+                        e[q] = t < t1 ? t + hd : -1;
+                        w[q] = hv;
+                    }
+                    int u[4];
 #pragma unroll
-                        for (int r = 0; r < kVT; ++r)
-                            if (valid[r] && u[r] != ws.aux[kk[r]] && scan_state(state, u[r]) != kOut)
-                                state[u[r]] = kOut;
-                    },
-                    NoPost());
+                    for (int q = 0; q < 4; ++q) u[q] = e[q] >= 0 ? __ldg(col + e[q]) : -1;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (u[q] >= 0 && u[q] != w[q]) mis_knock(a, u[q], check);
+                }
             }
             if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 2)) return;
         }
+        // the lists this round fills start empty; their slots were last read a round ago
+        if (gtid == 0) {
+            qlen[s2] = 0;
+            l1len[s1] = 0;
+            l2len[s1] = 0;
+            nlight[s1] = 0;
+            heavy[s1] = 0ull;
+        }
 
         // phase S: blocker checks, short scans and decisions, one thread per vertex; each
-        // step loads four neighbours at once and takes the first that decides anything
+        // scan step loads four neighbours at once and takes the first that decides anything
         {
-            WQ wq(sm.qbuf[wid][0], qn, qlen_next);
-            WQ wj(sm.qbuf[wid][1], a.joined, jlen_next);
+            WQ wq(qbuf[wid][0], qn, qlen + s1);
+            WQ wj(qbuf[wid][1], a.light, nlight + s0);
+            WQ wl(qbuf[wid][2], a.longq, l1len + s0);
             for (int base = blockIdx.x * kBlock; base < nf; base += gstride) {
                 const int i = base + threadIdx.x;
-                bool keep = false, joined = false;
+                bool keep = false, light = false, along = false;
                 int v = 0;
                 if (i < nf) {
-                    v = __ldcg(qc + i);
-                    if (__ldcg(state + v) == kUndecided) {
-                        const int r0 = __ldg(a.row_ptr + v), r1 = __ldg(a.row_ptr + v + 1);
-                        const int p = __ldcg(a.pos + v);
+                    // round 0 takes every vertex and writes every state: vertices without
+                    // neighbours join at once, the others start undecided with no blocker
+                    v = r == 0 ? i : __ldcg(qc + i);
+                    const int r0 = __ldg(a.row_ptr + v), r1 = __ldg(a.row_ptr + v + 1);
+                    if (r == 0 && r1 == r0) {
+                        state[v] = kIn;
+                    } else if (r == 0 || __ldcg(state + v) == kUndecided) {
+                        const int p = r == 0 ? r0 - 1 : __ldcg(a.pos + v);
+                        if (r == 0) state[v] = kUndecided;
                         if (p >= r0 && __ldcg(state + __ldg(col + p)) != kOut) {
-                            keep = true;  // its blocker is undecided, or joined (and pushes next round)
+                            keep = true;  // its blocker is undecided (or joined: its push comes next)
                         } else {
                             const unsigned pv = __ldg(a.prio + v);
                             const int start = p + 1, lim = min(r1, start + kMisThread);
@@ -986,7 +1025,7 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                                 for (int k = 0; k < 4; ++k) {
                                     pu[k] = __ldg(a.prio + u[k]);
                                     // in the first round every vertex with neighbours is undecided
-                                    su[k] = round == 1 ? kUndecided : scan_state(state, u[k]);
+                                    su[k] = r == 0 ? kUndecided : scan_state(state, u[k]);
                                 }
 #pragma unroll
                                 for (int k = 0; k < 4; ++k)
@@ -998,28 +1037,31 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                                 keep = true;
                                 a.pos[v] = stop;
                             } else if (lim >= r1) {
-                                joined = true;
                                 state[v] = kIn;
+                                light = r1 - r0 <= kMisLightRow;
+                                if (!light) mis_list_heavy(a, heavy + s0, v, r0, r1 - r0);
                             } else {  // settled up to lim - 1: a warp goes on
                                 a.pos[v] = lim - 1;
-                                a.longq[atomicAdd(l1len, 1)] = v;
+                                along = true;
                             }
                         }
                     }
                 }
                 wq.push(keep, v);
-                wj.push(joined, v);
+                wj.push(light, v);
+                wl.push(along, v);
             }
             wq.flush();
             wj.flush();
+            wl.flush();
         }
         if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 3)) return;
 
         // phase L: longer scans, one warp per vertex (up to kMisWarpChunks chunks of 32)
-        const int n1 = ld_volatile_i32(l1len);
+        const int n1 = ld_volatile_i32(l1len + s0);
         if (n1 > 0) {
-            WQ wq(sm.qbuf[wid][0], qn, qlen_next);
-            WQ wj(sm.qbuf[wid][1], a.joined, jlen_next);
+            WQ wq(qbuf[wid][0], qn, qlen + s1);
+            WQ wj(qbuf[wid][1], a.light, nlight + s0);
             const int gw = gtid >> 5, nw = gstride >> 5;
             for (int k = gw; k < n1; k += nw) {
                 const int v = __ldcg(a.longq + k);
@@ -1036,19 +1078,23 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                     }
                 }
                 const bool end = stop < 0 && start + 32 * c >= r1;
+                bool light = false;
                 if (lane == 0) {
                     scanned += min(r1, stop >= 0 ? stop + 1 : start + 32 * c) - start;
-                    if (stop >= 0)
+                    if (stop >= 0) {
                         a.pos[v] = stop;
-                    else if (end)
+                    } else if (end) {
                         state[v] = kIn;
-                    else {
+                        const int r0 = __ldg(a.row_ptr + v);
+                        light = r1 - r0 <= kMisLightRow;
+                        if (!light) mis_list_heavy(a, heavy + s0, v, r0, r1 - r0);
+                    } else {
                         a.pos[v] = start + 32 * kMisWarpChunks - 1;
-                        a.longq2[atomicAdd(l2len, 1)] = v;
+                        a.longq2[atomicAdd(l2len + s0, 1)] = v;
                     }
                 }
                 wq.push(stop >= 0 && lane == 0, v);
-                wj.push(end && lane == 0, v);
+                wj.push(light, v);
             }
             wq.flush();
             wj.flush();
@@ -1056,7 +1102,7 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
         }
 
         // phase L2: the longest scans, one block per vertex
-        const int n2 = n1 > 0 ? ld_volatile_i32(l2len) : 0;
+        const int n2 = n1 > 0 ? ld_volatile_i32(l2len + s0) : 0;
         if (n2 > 0) {
             for (int k = blockIdx.x; k < n2; k += G) {
                 const int v = __ldcg(a.longq2 + k);
@@ -1072,22 +1118,24 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                     if (__syncthreads_or(st)) break;
                 }
                 if (threadIdx.x == 0) {
-                    const int sp = s_stop;
-                    scanned += (sp != kInf ? sp + 1 : r1) - start;
-                    if (sp != kInf) {
-                        a.pos[v] = sp;
-                        qn[atomicAdd(qlen_next, 1)] = v;
+                    const int spos = s_stop;
+                    scanned += (spos != kInf ? spos + 1 : r1) - start;
+                    if (spos != kInf) {
+                        a.pos[v] = spos;
+                        qn[atomicAdd(qlen + s1, 1)] = v;
                     } else {
                         state[v] = kIn;
-                        a.joined[atomicAdd(jlen_next, 1)] = v;
+                        const int r0 = __ldg(a.row_ptr + v);
+                        if (r1 - r0 <= kMisLightRow)
+                            a.light[atomicAdd(nlight + s0, 1)] = v;
+                        else
+                            mis_list_heavy(a, heavy + s0, v, r0, r1 - r0);
                     }
                 }
                 __syncthreads();
             }
             if (!grid_barrier(a.ctl, a.sticky, kSiteMis + 5)) return;
         }
-        cur ^= 1;
-        jc ^= 1;
     }
     long long insz = 0;
     for (int i = gtid; i < m; i += gstride) {
@@ -1098,21 +1146,20 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
             a.member[i] = (s == kIn) ? 1 : 0;
         insz += (s == kIn);
     }
+    long long work = scanned + pushed;
     for (int o = 16; o; o >>= 1) {
         insz += __shfl_down_sync(0xffffffffu, insz, o);
-        scanned += __shfl_down_sync(0xffffffffu, scanned, o);
+        work += __shfl_down_sync(0xffffffffu, work, o);
     }
-    if ((threadIdx.x & 31) == 0 && insz)
+    if (lane == 0 && insz)
         atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->vertices_reached),
                   static_cast<unsigned long long>(insz));
-    if ((threadIdx.x & 31) == 0 && scanned)
+    if (lane == 0 && work)
         atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->edges_expanded),
-                  static_cast<unsigned long long>(scanned));
+                  static_cast<unsigned long long>(work));
     if (gtid == 0) {
-        a.ctl->iterations = round;
-        a.ctl->push_iterations = round;
-        atomicAdd(reinterpret_cast<unsigned long long *>(&a.ctl->edges_expanded),
-                  static_cast<unsigned long long>(expanded));
+        a.ctl->iterations = r;
+        a.ctl->push_iterations = r;
         a.ctl->edges_component = a.nnz;
     }
 }
@@ -1456,7 +1503,8 @@ static apspie_status mis_common(apspie_ctx *ctx, const apspie_csr *A, const uint
     if (!d_priority) return set_error(ctx, APSPIE_ERR_INVALID_ARG, "apspie_mis: NULL priority");
     void *base;
     const size_t tb = trav_scratch_bytes(A->m);
-    const size_t extra = Carver::need({static_cast<size_t>(A->m)});
+    const size_t mi = static_cast<size_t>(A->m) + 1;
+    const size_t extra = Carver::need({static_cast<size_t>(A->m), mi * 4, mi * 4});
     st = scratch_reserve(ctx, tb + extra, &base);
     if (st != APSPIE_OK) return st;
     if ((st = reset_ctl(ctx)) != APSPIE_OK) return st;
@@ -1468,13 +1516,23 @@ static apspie_status mis_common(apspie_ctx *ctx, const apspie_csr *A, const uint
     a.prio = d_priority;
     a.member = d_member;
     a.member_i32 = d_member_i32;
-    a.buf = carve_trav(base, A->m);
-    a.pos = a.buf.aux;
-    a.joined = a.buf.q3;
-    a.longq = a.buf.q2;
-    a.longq2 = a.buf.aux2;
+    const TravBuffers buf = carve_trav(base, A->m);
+    a.pos = buf.aux;
+    a.queue[0] = buf.q0;
+    a.queue[1] = buf.q1;
+    a.longq = buf.q2;
+    a.longq2 = buf.aux2;
+    a.heavy_v = buf.q3;
+    a.heavy_base = buf.rs;
+    a.heavy_delta = buf.loc_off;
     Carver c(static_cast<char *>(base) + tb);
     a.state = c.take<unsigned char>(A->m);
+    a.unit_owner = c.take<int>(mi);
+    a.light = c.take<int>(mi);
+    // push units hold at least 128 entries, and few enough that the units of a round's
+    // pushes (at most nnz entries) fit the m + 1 slots of unit_owner
+    a.unit_shift = 7;
+    while ((static_cast<long long>(A->nnz) >> a.unit_shift) + 1 > static_cast<long long>(mi)) ++a.unit_shift;
     a.ctl = ctx->d_ctl;
     a.sticky = ctx->d_sticky_err;
     void *args[] = {&a};

@@ -613,6 +613,10 @@ class Server:
     def set_sssp_min_batch(self, n: int) -> None:
         L.check(L.lib().apspie_server_set_sssp_min_batch(self.handle, n), None, "server_set_sssp_min_batch")
 
+    def set_side_room(self, on: bool) -> None:
+        """Persistent grids alone on the device leave room for small kernels (default on)."""
+        L.check(L.lib().apspie_server_set_side_room(self.handle, int(bool(on))), None, "server_set_side_room")
+
     def start(self) -> None:
         L.check(L.lib().apspie_server_start(self.handle), None, "server_start")
 
@@ -622,6 +626,21 @@ class Server:
                 None, "server_submit")
         return t.value
 
+    def submit_many(self, graph_ids, kinds, sources, outs) -> np.ndarray:
+        """Queues len(outs) requests at once (one lock, one worker wake-up); returns their
+        tickets. Nothing is queued if any request is invalid."""
+        n = len(outs)
+        g = np.ascontiguousarray(graph_ids, dtype=np.int32)
+        k = np.ascontiguousarray(kinds, dtype=np.int32)
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        ptrs = np.array([o.data_ptr() for o in outs], dtype=np.uint64)
+        if not (len(g) == len(k) == len(src) == n):
+            raise ValueError("submit_many: graph_ids, kinds, sources and outs differ in length")
+        t = np.zeros(n, dtype=np.uint64)
+        L.check(L.lib().apspie_server_submit_many(self.handle, n, g.ctypes.data, k.ctypes.data, src.ctypes.data,
+                                                  ptrs.ctypes.data, t.ctypes.data), None, "server_submit_many")
+        return t
+
     def wait(self, ticket: int, timeout_ms: int = 600000) -> float:
         lat = ctypes.c_double()
         L.check(L.lib().apspie_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(lat)), None, "server_wait")
@@ -629,9 +648,11 @@ class Server:
 
     def take_completed(self, cap: int = 1024, timeout_ms: int = 600000):
         """[(ticket, status, latency_ms)] of requests completed since the last call (>= 1)."""
-        t = np.zeros(cap, dtype=np.uint64)
-        stv = np.zeros(cap, dtype=np.int32)
-        lat = np.zeros(cap, dtype=np.float64)
+        if getattr(self, "_take_cap", 0) < cap:  # result buffers, reused across calls
+            self._take_cap = cap
+            self._take_buf = (np.zeros(cap, dtype=np.uint64), np.zeros(cap, dtype=np.int32),
+                              np.zeros(cap, dtype=np.float64))
+        t, stv, lat = self._take_buf
         n = ctypes.c_int32()
         L.check(L.lib().apspie_server_take_completed(self.handle, timeout_ms, cap, t.ctypes.data, stv.ctypes.data,
                                                      lat.ctypes.data, ctypes.byref(n)), None, "server_take_completed")

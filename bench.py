@@ -724,12 +724,13 @@ def serve_plain(ctx, dgs, prios, stream, dev, hasher=None):
     return lat, total
 
 
-def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None):
+def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None, pool_rows=None, side_room=True):
     """The same stream through apspie_server (40 GB budget): the main thread submits at the
     arrival times from a pool of output rows per graph and, whenever a pool runs dry or
     while it waits for the next arrival, takes completed requests in bulk, hashes their
     rows on the device and returns the rows to the pools. Latency = server latency (submit
-    to completion) + how late the submit was after the arrival."""
+    to completion) + how late the submit was after the arrival. pool_rows: int32 output
+    rows per graph (default POOL_ROWS each)."""
     import torch
 
     import apspie_b200 as ap
@@ -737,15 +738,17 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None):
     kinds, which, srcs, arrive = stream
     srv = ap.Server(int(dev.split(":")[1]), budget_bytes=40 << 30, slots=slots or SERVE_SLOTS,
                     max_batch=max_batch or SERVE_MAX_BATCH)
+    srv.set_side_room(side_room)
     gids = [srv.add_graph(g) for g in graphs]
     srv.start()
-    pools = [[torch.empty(g.m, dtype=torch.int32, device=dev) for _ in range(POOL_ROWS)] for g in graphs]
+    pool_rows = pool_rows or [POOL_ROWS] * len(graphs)
+    pools = [[torch.empty(g.m, dtype=torch.int32, device=dev) for _ in range(k)] for g, k in zip(graphs, pool_rows)]
     mpools = [[torch.empty(g.m, dtype=torch.uint8, device=dev) for _ in range(64)] for g in graphs]
     # warm-up: a burst of every (graph, kind) before the clock starts
     warm = []
     for gi, g in enumerate(graphs):
         for kind in (0, 1, 2):
-            for k in range(16):
+            for k in range(min(16, len(pools[gi]))):
                 o = (mpools if kind == 2 else pools)[gi][k]
                 warm.append(srv.submit(gids[gi], kind, (k * 7919 + 1) % g.m, o))
     for t in warm:
@@ -755,15 +758,23 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None):
     late = np.zeros(n)
     lat = np.zeros(n)
     hashed = []  # rows hashed since the last stream sync (returned to pools after it)
+    # where the client's time goes: submit calls, waits for completions (blocking takes),
+    # and checking (hashing the completed rows and syncing before their rows are reused)
+    client = {"submit_s": 0.0, "wait_s": 0.0, "check_s": 0.0, "blocking_takes": 0, "pool_empty": 0}
 
     def drain(block):
         got = []
         if owner:
+            t_w = time.perf_counter()
             try:
                 got = srv.take_completed(cap=4096, timeout_ms=-1 if block else 0)
             except ap.ApspieError as e:
                 if e.name != "APSPIE_ERR_TIMEOUT":
                     raise
+            if block:
+                client["wait_s"] += time.perf_counter() - t_w
+                client["blocking_takes"] += 1
+        t_c = time.perf_counter()
         for t, status, ms in got:
             i, row, pool = owner.pop(t)
             if status != 0:
@@ -777,29 +788,50 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None):
             for row, pool in hashed:
                 pool.append(row)
             hashed.clear()
+        client["check_s"] += time.perf_counter() - t_c
         return len(got)
 
+    gid_of = np.asarray(gids, dtype=np.int32)[np.asarray(which, dtype=np.int64)]
     t0 = time.perf_counter()
-    for i in range(n):
-        k, w, s = int(kinds[i]), int(which[i]), int(srcs[i])
-        while time.perf_counter() - t0 < arrive[i]:
-            if drain(False) == 0:
-                time.sleep(min(2e-4, max(0.0, arrive[i] - (time.perf_counter() - t0))))
-        pool = mpools[w] if k == 2 else pools[w]
-        while not pool:
-            drain(True)
-        row = pool.pop()
+    i = 0
+    next_note = 20000
+    while i < n:
         now = time.perf_counter() - t0
-        late[i] = (now - arrive[i]) * 1e3
-        owner[srv.submit(gids[w], k, s, row)] = (i, row, pool)
-        if i % 20000 == 19999:
-            _progress(f"server: {i + 1} submitted, {i + 1 - len(owner)} completed")
+        if arrive[i] > now:
+            if drain(False) == 0:
+                time.sleep(min(2e-4, max(0.0, arrive[i] - now)))
+            continue
+        # every request that has arrived and has an output row, in arrival order, is
+        # submitted in one call
+        batch, rows, bpools = [], [], []
+        while i < n and arrive[i] <= now and len(batch) < 4096:
+            pool = mpools[int(which[i])] if int(kinds[i]) == 2 else pools[int(which[i])]
+            if not pool:
+                break
+            rows.append(pool.pop())
+            bpools.append(pool)
+            batch.append(i)
+            i += 1
+        if not batch:
+            client["pool_empty"] += 1
+            drain(True)
+            continue
+        t_s = time.perf_counter()
+        late[batch] = (t_s - t0 - np.asarray(arrive)[batch]) * 1e3
+        tickets = srv.submit_many(gid_of[batch], np.asarray(kinds)[batch], np.asarray(srcs)[batch], rows)
+        for t, j, row, pool in zip(tickets.tolist(), batch, rows, bpools):
+            owner[t] = (j, row, pool)
+        client["submit_s"] += time.perf_counter() - t_s
+        if i >= next_note:
+            _progress(f"server: {i} submitted, {i - len(owner)} completed")
+            next_note += 20000
     while owner:
         drain(True)
     total = time.perf_counter() - t0
     torch.cuda.synchronize()
     st = srv.stats()
     srv.close()
+    st["client"] = {k: round(v, 4) if isinstance(v, float) else v for k, v in client.items()}
     return lat, total, st
 
 
@@ -820,32 +852,39 @@ def extras_serving(ctx, args, local, g22):
     prios = [torch.from_numpy(ap.mt19937_u32(4, g.m).view(np.int32)).to(dev) for g in graphs]
     n = args.serve_queries
     m_max = max(g.m for g in graphs)
-    sat = serve_stream(graphs, n, 0.0)
-    serve_plain(ctx, dgs, prios, serve_stream(graphs, 50, 0.0), dev)  # warm-up
-    ref = RowHasher(ctx, m_max, n, dev)
-    _progress(f"serving: plain path, {n} queries")
-    lat_p, tot_p = serve_plain(ctx, dgs, prios, sat, dev, ref)
-    ref_h = ref.result()
-    plain_qps = n / tot_p
+    legs = set(args.serve_legs.split(","))
     hctx = ap.Context(local)  # the server leg's checksums run on torch's current stream
-
-    def run_server(stream):
-        _progress("serving: server")
-        h = RowHasher(hctx, m_max, n, dev, ref.coef)
-        lat_s, tot_s, st = serve_server(graphs, stream, dev, h)
-        return lat_s, tot_s, st, int((h.result() == ref_h).sum())
-
-    lat_s, tot_s, st, same = run_server(sat)
     res = {"serving": {
         "workload": "4 graphs R-MAT s16/s18/s20/s22, 70/25/5 BFS/SSSP/MIS, 40 GB budget, 100,000 queries",
-        "slots": SERVE_SLOTS, "max_batch": SERVE_MAX_BATCH,
-        "queries": n, "plain_qps": plain_qps, "server_qps": n / tot_s, "x_plain": tot_p / tot_s,
-        "saturated": {"server": _pct(lat_s), "plain": _pct(lat_p)},
-        "launches": st["launches"], "joined_running": st["joined_running"], "trivial": st["trivial"],
-        "engine_launches": st["engine_launches"], "engine_levels": st["engine_levels"],
-        "max_batch_seen": st["max_batch_seen"], "peak_bytes": st["peak_bytes"],
-        "exact_checked": n, "exact_equal": same, "exact": same == n}}
-    for mult in (0.8, 2.0):
+        "slots": SERVE_SLOTS, "max_batch": SERVE_MAX_BATCH, "queries": n}}
+    coef = None
+    if legs & {"mixed", "poisson"}:
+        sat = serve_stream(graphs, n, 0.0)
+        serve_plain(ctx, dgs, prios, serve_stream(graphs, 50, 0.0), dev)  # warm-up
+        ref = RowHasher(ctx, m_max, n, dev)
+        coef = ref.coef
+        _progress(f"serving: plain path, {n} queries")
+        lat_p, tot_p = serve_plain(ctx, dgs, prios, sat, dev, ref)
+        ref_h = ref.result()
+        plain_qps = n / tot_p
+
+        def run_server(stream):
+            _progress("serving: server")
+            h = RowHasher(hctx, m_max, n, dev, ref.coef)
+            lat_s, tot_s, st = serve_server(graphs, stream, dev, h, side_room=not args.serve_no_side_room)
+            return lat_s, tot_s, st, int((h.result() == ref_h).sum())
+
+    if "mixed" in legs:
+        lat_s, tot_s, st, same = run_server(sat)
+        res["serving"].update({
+            "plain_qps": plain_qps, "server_qps": n / tot_s, "x_plain": tot_p / tot_s,
+            "saturated": {"server": _pct(lat_s), "plain": _pct(lat_p)},
+            "launches": st["launches"], "joined_running": st["joined_running"], "trivial": st["trivial"],
+            "engine_launches": st["engine_launches"], "engine_levels": st["engine_levels"],
+            "client": st["client"],
+            "max_batch_seen": st["max_batch_seen"], "peak_bytes": st["peak_bytes"],
+            "exact_checked": n, "exact_equal": same, "exact": same == n})
+    for mult in ((0.8, 2.0) if "poisson" in legs else ()):
         rate = mult * plain_qps
         stream = serve_stream(graphs, n, rate)
         lat_s, tot_s, st, same = run_server(stream)
@@ -855,16 +894,20 @@ def extras_serving(ctx, args, local, g22):
             "rate_qps": rate, "server": dict(_pct(lat_s), qps=n / tot_s),
             "plain": dict(_pct(lat_p), qps=n / tot_p), "joined_running": st["joined_running"],
             "exact_checked": n, "exact": same == n}
+    if "bfs" not in legs:
+        hctx.close()
+        return res
     # BFS-only stream on the scale-22 graph: the batched-serving target
     words = ap.mt19937_u32(8, n).astype(np.int64)
     bstream = (np.zeros(n, dtype=int), np.full(n, 3), words % graphs[3].m, np.zeros(n))
-    bref = RowHasher(ctx, m_max, n, dev, ref.coef)
+    bref = RowHasher(ctx, m_max, n, dev, coef)
     _progress("serving: BFS-only stream, plain path")
     lat_p, tot_p = serve_plain(ctx, dgs, prios, bstream, dev, bref)
     _progress("serving: BFS-only stream, server")
     bref_h = bref.result()
-    h = RowHasher(hctx, m_max, n, dev, ref.coef)
-    lat_s, tot_s, st = serve_server(graphs, bstream, dev, h)
+    h = RowHasher(hctx, m_max, n, dev, bref.coef)
+    pool = [0] * (len(graphs) - 1) + [args.serve_pool]  # only the scale-22 graph is queried
+    lat_s, tot_s, st = serve_server(graphs, bstream, dev, h, pool_rows=pool, side_room=not args.serve_no_side_room)
     same = int((h.result() == bref_h).sum())
     hctx.close()
     res["serving"]["bfs_only_rmat22_saturated"] = {
@@ -872,6 +915,7 @@ def extras_serving(ctx, args, local, g22):
         "server": _pct(lat_s), "plain": _pct(lat_p), "launches": st["launches"],
         "joined_running": st["joined_running"], "trivial": st["trivial"], "max_batch_seen": st["max_batch_seen"],
         "engine_launches": st["engine_launches"], "engine_levels": st["engine_levels"],
+        "client": st["client"], "pool_rows": args.serve_pool, "side_room": not args.serve_no_side_room,
         "exact_checked": n, "exact": same == n}
     return res
 
@@ -886,6 +930,12 @@ def main():
     ap_.add_argument("--no-cpu-baseline", action="store_true")
     ap_.add_argument("--serve-queries", type=int, default=SERVE_QUERIES,
                      help="length of the serving streams (default: the config's 100,000)")
+    ap_.add_argument("--serve-pool", type=int, default=4096,
+                     help="output rows the BFS-only serving leg keeps in flight")
+    ap_.add_argument("--serve-no-side-room", action="store_true",
+                     help="serving: let a slot's persistent grid fill the device when it runs alone")
+    ap_.add_argument("--serve-legs", default="mixed,poisson,bfs",
+                     help="serving legs to run (comma list of mixed, poisson, bfs)")
     ap_.add_argument("--only-extra", choices=["traversal", "spgemm_tc", "build", "batched", "serving"], default=None,
                      help="run one extra leg alone and print its JSON (no headline line)")
     args = ap_.parse_args()

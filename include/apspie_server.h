@@ -69,12 +69,23 @@ apspie_status apspie_server_set_bfs_min_batch(apspie_server *s, int32_t min_batc
  * scale 16, 8 at scale 18), larger graphs never (a slot's multi-query launch holds only
  * its share of the SMs, while single-source queries spread over all slots). */
 apspie_status apspie_server_set_sssp_min_batch(apspie_server *s, int32_t min_batch);
+/* on != 0 (default): a slot's persistent grid that has the device to itself takes fewer
+ * blocks per SM, so that 4096 registers per SM stay free for small kernels of other
+ * streams (the answers for sources without edges, the caller's own kernels); 0: it fills
+ * the device. Before start. */
+apspie_status apspie_server_set_side_room(apspie_server *s, int32_t on);
 /* Reserves the slots' scratch and starts the worker thread. */
 apspie_status apspie_server_start(apspie_server *s);
 /* Queues a request; the answer is written to d_out (device memory of the server's GPU),
  * which must stay valid until the request completes. Thread-safe. */
 apspie_status apspie_server_submit(apspie_server *s, int32_t graph_id, int32_t kind, int32_t source,
                                    void *d_out, uint64_t *ticket);
+/* Queues n requests at once (request i: graph_ids[i], kinds[i], sources[i], d_outs[i]; its
+ * ticket in tickets[i]), under one lock and with one wake-up of the worker. Every request
+ * is checked first: if any is invalid, none is queued and the status is the one
+ * apspie_server_submit would return for the first invalid request. Thread-safe. */
+apspie_status apspie_server_submit_many(apspie_server *s, int32_t n, const int32_t *graph_ids, const int32_t *kinds,
+                                        const int32_t *sources, void *const *d_outs, uint64_t *tickets);
 /* Blocks until the request completes (timeout_ms < 0: no limit); returns its status and
  * the latency from submit to completion in *latency_ms. A ticket can be waited once. */
 apspie_status apspie_server_wait(apspie_server *s, uint64_t ticket, int32_t timeout_ms,

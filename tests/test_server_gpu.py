@@ -179,3 +179,70 @@ def test_server_take_completed_reports_each_request_once(ctx, graphs):
     with pytest.raises(ap.ApspieError):
         srv.wait(tickets[0], timeout_ms=10)  # already reported
     srv.close()
+
+
+def test_server_submit_many_matches_single_submits(ctx, graphs):
+    """A mixed batch submitted in one call: every answer equals the plain path's; a batch
+    holding one invalid request is rejected whole (nothing of it runs)."""
+    g = graphs[1]
+    srv = ap.Server(0, budget_bytes=2 << 30, slots=2, max_batch=64)
+    gid = srv.add_graph(g)
+    srv.start()
+    kinds = [L.QUERY_BFS] * 40 + [L.QUERY_SSSP] * 10 + [L.QUERY_MIS] * 3
+    srcs = [(13 * i + 5) % g.m for i in range(len(kinds))]
+    outs = [_out(g, k) for k in kinds]
+    bad = list(srcs)
+    bad[7] = g.m  # out of range
+    with pytest.raises(ap.ApspieError):
+        srv.submit_many([gid] * len(kinds), kinds, bad, outs)
+    tickets = srv.submit_many([gid] * len(kinds), kinds, srcs, outs)
+    assert len(set(tickets.tolist())) == len(kinds)
+    done = set()
+    while len(done) < len(kinds):
+        for t, status, _ in srv.take_completed():
+            assert status == 0
+            done.add(t)
+    st = srv.stats()
+    srv.close()
+    assert done == set(tickets.tolist())
+    assert st["submitted"] == len(kinds) and st["completed"] == len(kinds)
+    for k, s_, o in zip(kinds, srcs, outs):
+        np.testing.assert_array_equal(o.cpu().numpy(), _plain(ctx, g, k, int(s_)), err_msg=f"{k} {s_}")
+
+
+def test_server_sources_without_edges_any_row_alignment(ctx):
+    """Sources without edges are answered by the side kernel (every entry -1 but the
+    source's 0): rows of a length that is not a multiple of 4, rows that start off a
+    16-byte boundary, and sources at every position of a 4-entry group."""
+    import torch
+
+    m = 1001
+    rng = np.random.default_rng(5)
+    edges = {(int(a), int(b)) for a, b in rng.integers(0, 500, (800, 2)) if a != b}  # 500..1000 isolated
+    rows = [[] for _ in range(m)]
+    for a, b in edges:
+        rows[a].append(b)
+        rows[b].append(a)
+    rp = np.zeros(m + 1, dtype=np.int32)
+    for v in range(m):
+        rp[v + 1] = rp[v] + len(set(rows[v]))
+    ci = np.concatenate([np.array(sorted(set(r)), dtype=np.int32) for r in rows if r] or [np.zeros(0, np.int32)])
+    g = ap.HostGraph(m, m, rp, ci, None, True)
+    srv = ap.Server(0, budget_bytes=1 << 30, slots=1)
+    gid = srv.add_graph(g)
+    srv.start()
+    srcs = [996, 997, 998, 999, 1000] + [600, 601, 602, 603, 1000]
+    big = torch.empty(5 * (m + 1) + 4, dtype=torch.int32, device="cuda")
+    outs = [big[1 + k * (m + 1):1 + k * (m + 1) + m] for k in range(5)]  # views off a 16-byte boundary
+    outs += [torch.empty(m, dtype=torch.int32, device="cuda") for _ in range(5)]  # aligned rows
+    tickets = [srv.submit(gid, L.QUERY_BFS, s_, o) for s_, o in zip(srcs, outs)]
+    for t in tickets:
+        srv.wait(t)
+    st = srv.stats()
+    srv.close()
+    assert st["trivial"] == len(srcs)
+    for s_, o in zip(srcs, outs):
+        want = np.full(m, -1, dtype=np.int32)
+        want[s_] = 0
+        np.testing.assert_array_equal(o.cpu().numpy(), want, err_msg=str(s_))
+

@@ -89,3 +89,9 @@ def test_row_checksums_match_a_torch_computation(ctx):
     o8 = torch.zeros(3, dtype=torch.int64, device="cuda")
     ctx.row_checksums(u8, [0, 1, 2], coef, o8)
     assert torch.equal(o8, torch.stack([torch.sum(r.to(torch.int32) * coef, dtype=torch.int64) for r in u8]))
+    # int32 rows starting off a 16-byte boundary (views at 4-byte offsets) take the scalar path
+    big = torch.randint(-1, 40, (m + 3,), generator=g, dtype=torch.int32).cuda()
+    views = [big[k:k + m] for k in (1, 2, 3)]
+    ov = torch.zeros(3, dtype=torch.int64, device="cuda")
+    ctx.row_checksums(views, [0, 1, 2], coef, ov)
+    assert torch.equal(ov, torch.stack([torch.sum(r * coef, dtype=torch.int64) for r in views]))
