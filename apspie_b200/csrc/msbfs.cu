@@ -41,7 +41,8 @@ constexpr int kHeavyDeg = 128;  // pull: rows longer than this are scanned by a 
 // The engine is the same kernel with SERVE = true: instead of a fixed set of sources it
 // keeps 32 * W query slots and, at the start of every level, block 0 retires the queries
 // whose frontier died in the previous level (posting their ids to the host), then admits
-// requests the host posted into a ring in host-mapped memory into free slots. An admitted
+// requests the host posted into a ring in host-mapped memory into free slots, while at most
+// 1/kAdmitFrac of the slots are in flight (so that queries run in generations). An admitted
 // query starts at that level (its depths are level - start), its output row is filled in
 // the same level's first phase, and it runs alongside the queries already in flight. A
 // retired slot keeps its visited bits until a sweep clears them; only swept slots are
@@ -49,6 +50,10 @@ constexpr int kHeavyDeg = 128;  // pull: rows longer than this are scanned by a 
 // stopped admission); the host relaunches it when requests arrive later. Nothing on the
 // device waits for the host: the ring is read once per level.
 constexpr int kServeRing = 4096;  // request and completion ring entries
+#ifndef APSPIE_ADMIT_FRAC
+#define APSPIE_ADMIT_FRAC 8
+#endif
+constexpr int kAdmitFrac = APSPIE_ADMIT_FRAC;  // admissions while at most 1/kAdmitFrac of the slots are in flight
 constexpr int kServeSlots = 512;  // upper bound of 32 * W
 
 struct ServeRequest {
@@ -171,10 +176,21 @@ __device__ void serve_admin(const MsArgs &a, int L, int cur) {
         const unsigned long long tail = ld_acquire_sys_u64(&mb->tail);
         const int accept = mb->accept && L < a.max_levels;
         const unsigned long long head = sv->head;
-        int free_clean = 0;
-        for (int w = 0; w < W; ++w) free_clean += __popc(~(s_act[w] | s_dirty[w]));
+        int free_clean = 0, in_flight = 0;
+        for (int w = 0; w < W; ++w) {
+            free_clean += __popc(~(s_act[w] | s_dirty[w]));
+            in_flight += __popc(s_act[w]);
+        }
+        // new queries join only while at most 1/kAdmitFrac of the slots are in flight, so
+        // that queries run in generations that start (nearly) together: their frontiers
+        // grow and shrink together, and a bottom-up level serves them all. Queries started
+        // at every level would keep some frontier small at every level, and the bottom-up
+        // scans would read whole rows for them level after level.
+        const bool gate = in_flight * kAdmitFrac <= Q;
         const unsigned long long waiting = tail > head ? tail - head : 0ull;
-        s_nadm = accept ? static_cast<int>(waiting < static_cast<unsigned long long>(free_clean) ? waiting : free_clean) : 0;
+        s_nadm = accept && gate
+                     ? static_cast<int>(waiting < static_cast<unsigned long long>(free_clean) ? waiting : free_clean)
+                     : 0;
         s_head = head;
         s_tail = tail;
         s_accept = accept;
