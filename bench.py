@@ -16,6 +16,7 @@ process per step on every host core it may use.
 from __future__ import annotations
 
 import argparse
+import collections
 import json
 import os
 import statistics
@@ -757,10 +758,27 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None, pool_r
     owner = {}  # ticket -> (query index, row tensor, pool)
     late = np.zeros(n)
     lat = np.zeros(n)
-    hashed = []  # rows hashed since the last stream sync (returned to pools after it)
+    hashed = []  # rows whose checksums are queued but not yet launched as a group
+    checks = collections.deque()  # (event after a group's checksums, its (row, pool) pairs)
     # where the client's time goes: submit calls, waits for completions (blocking takes),
-    # and checking (hashing the completed rows and syncing before their rows are reused)
-    client = {"submit_s": 0.0, "wait_s": 0.0, "check_s": 0.0, "blocking_takes": 0, "pool_empty": 0}
+    # hashing the completed rows, and waits for checksums before their rows are reused
+    client = {"submit_s": 0.0, "wait_s": 0.0, "check_s": 0.0, "check_wait_s": 0.0, "blocking_takes": 0,
+              "pool_empty": 0}
+
+    def recycle(wait):
+        """Rows whose checksums have run go back to their pools (wait: for the oldest group)."""
+        back = 0
+        while checks and (wait or checks[0][0].query()):
+            ev, done = checks.popleft()
+            if wait:
+                t_w = time.perf_counter()
+                ev.synchronize()
+                client["check_wait_s"] += time.perf_counter() - t_w
+                wait = False
+            for row, pool in done:
+                pool.append(row)
+            back += len(done)
+        return back
 
     def drain(block):
         got = []
@@ -783,11 +801,13 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None, pool_r
             hasher.put(i, row)
             hashed.append((row, pool))
         if hashed and (block or len(hashed) >= 256):
+            # the rows return to their pools once the event after their checksums has passed
             hasher.flush()
-            torch.cuda.current_stream().synchronize()
-            for row, pool in hashed:
-                pool.append(row)
+            ev = torch.cuda.Event()
+            ev.record(torch.cuda.current_stream())
+            checks.append((ev, list(hashed)))
             hashed.clear()
+        recycle(False)
         client["check_s"] += time.perf_counter() - t_c
         return len(got)
 
@@ -814,7 +834,12 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None, pool_r
             i += 1
         if not batch:
             client["pool_empty"] += 1
-            drain(True)
+            if not recycle(False):
+                if owner:
+                    drain(True)
+                else:
+                    drain(True)  # nothing at the server: launch the queued rows' checksums
+                    recycle(True)
             continue
         t_s = time.perf_counter()
         late[batch] = (t_s - t0 - np.asarray(arrive)[batch]) * 1e3
@@ -827,6 +852,9 @@ def serve_server(graphs, stream, dev, hasher, slots=None, max_batch=None, pool_r
             next_note += 20000
     while owner:
         drain(True)
+    drain(True)
+    while checks:
+        recycle(True)
     total = time.perf_counter() - t0
     torch.cuda.synchronize()
     st = srv.stats()

@@ -1,7 +1,7 @@
 """A CPU model of the server's BFS engine protocol (msbfs_kernel with SERVE = true): query
 slots, per-level retirement of queries whose frontier died, admission of waiting requests
-into swept slots (while at most 1/8 of the slots are in flight: queries run in
-generations), depths relative to each query's start level. Requests arrive at random
+into swept slots (while at most 1/admit_frac of the slots are in flight -- the kernel uses
+1/32: queries run in generations), depths relative to each query's start level. Requests arrive at random
 levels; every completed row must equal the oracle's BFS from its source, each request
 must complete exactly once, and models with a planted mistake must fail. No GPU."""
 import numpy as np
@@ -13,10 +13,7 @@ from test_batch_sssp_model import _random_graph
 Q = 32  # one word of query slots
 
 
-ADMIT_FRAC = 8  # admissions while at most Q / ADMIT_FRAC queries are in flight
-
-
-def _run_engine(rp, ci, arrivals, sweep=True, check_alive=True, max_levels=10_000, gate=True):
+def _run_engine(rp, ci, arrivals, sweep=True, check_alive=True, max_levels=10_000, gate=True, admit_frac=32):
     """arrivals: list of (level, source). Returns {request index: (completion level, row)}."""
     n = len(rp) - 1
     full = (1 << Q) - 1
@@ -49,7 +46,7 @@ def _run_engine(rp, ci, arrivals, sweep=True, check_alive=True, max_levels=10_00
                 r = slot_req.pop(s)
                 done[r] = (L, list(rows[r]))  # what the host reads at completion
         free = ~(act | dirty) & full if sweep else ~act & full
-        if gate and bin(act).count("1") * ADMIT_FRAC > Q:
+        if gate and bin(act).count("1") * admit_frac > Q:
             free = 0  # a generation is still running: arrivals wait for it to drain
         while waiting and free:
             s = (free & -free).bit_length() - 1
@@ -103,14 +100,14 @@ def _stream(rng, n, count, spread):
     return [(int(rng.integers(0, spread)), int(rng.integers(0, n))) for _ in range(count)]
 
 
-@pytest.mark.parametrize("gate", [True, False])
+@pytest.mark.parametrize("gate,admit_frac", [(True, 32), (True, 8), (False, 32)])
 @pytest.mark.parametrize("seed", range(6))
-def test_engine_rows_equal_single_source_bfs(seed, gate):
+def test_engine_rows_equal_single_source_bfs(seed, gate, admit_frac):
     rng = np.random.default_rng(100 + seed)
     rp, ci, _ = _random_graph(rng, int(rng.integers(20, 60)), int(rng.integers(1, 4)))
     n = len(rp) - 1
     arrivals = _stream(rng, n, 90, 25)  # more requests than slots, arriving over 25 levels
-    done = _run_engine(rp, ci, arrivals, gate=gate)
+    done = _run_engine(rp, ci, arrivals, gate=gate, admit_frac=admit_frac)
     assert sorted(done) == list(range(len(arrivals)))
     for r, (lvl, row) in done.items():
         ref = oracle.bfs(rp, ci, arrivals[r][1])
