@@ -785,8 +785,14 @@ __global__ void __launch_bounds__(kBlock, APSPIE_SSSP_MINB) sssp_group_kernel(Ss
 // MIS
 // ================================================================================
 enum : unsigned char { kUndecided = 0, kIn = 1, kOut = 2 };
-constexpr int kMisThread = 16;     // neighbours one thread scans (phase S) before handing the vertex on
-constexpr int kMisWarpChunks = 8;  // chunks of 32 neighbours a warp scans (phase L) before handing on
+#ifndef APSPIE_MIS_THREAD
+#define APSPIE_MIS_THREAD 16
+#endif
+#ifndef APSPIE_MIS_WARP_CHUNKS
+#define APSPIE_MIS_WARP_CHUNKS 8
+#endif
+constexpr int kMisThread = APSPIE_MIS_THREAD;          // neighbours one thread scans (phase S) before handing on
+constexpr int kMisWarpChunks = APSPIE_MIS_WARP_CHUNKS;  // chunks of 32 neighbours a warp scans (phase L)
 constexpr int kMisLightRow = 64;   // joiners with at most this many neighbours push by one thread
 
 struct MisArgs {

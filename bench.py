@@ -884,7 +884,7 @@ def extras_serving(ctx, args, local, g22):
     hctx = ap.Context(local)  # the server leg's checksums run on torch's current stream
     res = {"serving": {
         "workload": "4 graphs R-MAT s16/s18/s20/s22, 70/25/5 BFS/SSSP/MIS, 40 GB budget, 100,000 queries",
-        "slots": SERVE_SLOTS, "max_batch": SERVE_MAX_BATCH, "queries": n}}
+        "slots": args.serve_slots, "max_batch": SERVE_MAX_BATCH, "queries": n}}
     coef = None
     if legs & {"mixed", "poisson"}:
         sat = serve_stream(graphs, n, 0.0)
@@ -899,7 +899,8 @@ def extras_serving(ctx, args, local, g22):
         def run_server(stream):
             _progress("serving: server")
             h = RowHasher(hctx, m_max, n, dev, ref.coef)
-            lat_s, tot_s, st = serve_server(graphs, stream, dev, h, side_room=not args.serve_no_side_room)
+            lat_s, tot_s, st = serve_server(graphs, stream, dev, h, slots=args.serve_slots,
+                                            side_room=not args.serve_no_side_room)
             return lat_s, tot_s, st, int((h.result() == ref_h).sum())
 
     if "mixed" in legs:
@@ -935,7 +936,8 @@ def extras_serving(ctx, args, local, g22):
     bref_h = bref.result()
     h = RowHasher(hctx, m_max, n, dev, bref.coef)
     pool = [0] * (len(graphs) - 1) + [args.serve_pool]  # only the scale-22 graph is queried
-    lat_s, tot_s, st = serve_server(graphs, bstream, dev, h, pool_rows=pool, side_room=not args.serve_no_side_room)
+    lat_s, tot_s, st = serve_server(graphs, bstream, dev, h, slots=args.serve_slots, pool_rows=pool,
+                                    side_room=not args.serve_no_side_room)
     same = int((h.result() == bref_h).sum())
     hctx.close()
     res["serving"]["bfs_only_rmat22_saturated"] = {
@@ -958,6 +960,7 @@ def main():
     ap_.add_argument("--no-cpu-baseline", action="store_true")
     ap_.add_argument("--serve-queries", type=int, default=SERVE_QUERIES,
                      help="length of the serving streams (default: the config's 100,000)")
+    ap_.add_argument("--serve-slots", type=int, default=SERVE_SLOTS, help="server execution slots")
     ap_.add_argument("--serve-pool", type=int, default=4096,
                      help="output rows the BFS-only serving leg keeps in flight")
     ap_.add_argument("--serve-no-side-room", action="store_true",
