@@ -51,7 +51,7 @@ constexpr int kHeavyDeg = 128;  // pull: rows longer than this are scanned by a 
 // device waits for the host: the ring is read once per level.
 constexpr int kServeRing = 4096;  // request and completion ring entries
 #ifndef APSPIE_ADMIT_FRAC
-#define APSPIE_ADMIT_FRAC 32
+#define APSPIE_ADMIT_FRAC 64
 #endif
 constexpr int kAdmitFrac = APSPIE_ADMIT_FRAC;  // admissions while at most 1/kAdmitFrac of the slots are in flight
 constexpr int kServeSlots = 512;  // upper bound of 32 * W

@@ -1,7 +1,7 @@
 """A CPU model of the server's BFS engine protocol (msbfs_kernel with SERVE = true): query
 slots, per-level retirement of queries whose frontier died, admission of waiting requests
 into swept slots (while at most 1/admit_frac of the slots are in flight -- the kernel uses
-1/32: queries run in generations), depths relative to each query's start level. Requests arrive at random
+1/64: queries run in generations), depths relative to each query's start level. Requests arrive at random
 levels; every completed row must equal the oracle's BFS from its source, each request
 must complete exactly once, and models with a planted mistake must fail. No GPU."""
 import numpy as np
