@@ -826,7 +826,12 @@ __device__ __forceinline__ bool outranks(unsigned pu, int u, unsigned pv, int v)
 // safe: states only move from undecided to in or out, so a stale read can only make a scan
 // stop early at a neighbour that is already out, and the next round's blocker check (a
 // coherent read) sees it out and resumes the scan behind it.
-__device__ __forceinline__ unsigned char scan_state(const unsigned char *state, int u) { return state[u]; }
+#ifndef APSPIE_MIS_STATE_STRIDE
+#define APSPIE_MIS_STATE_STRIDE 1
+#endif
+constexpr int kMisStateStride = APSPIE_MIS_STATE_STRIDE;  // bytes between consecutive vertices' states
+__device__ __forceinline__ long long sx(int v) { return static_cast<long long>(v) * kMisStateStride; }
+__device__ __forceinline__ unsigned char scan_state(const unsigned char *state, int u) { return state[sx(u)]; }
 
 // One neighbour of a scanning vertex v: does it decide anything (an outranking neighbour
 // that is not out: v's new blocker, or -- if in -- the vertex that knocks v out)?
@@ -842,7 +847,7 @@ __device__ __forceinline__ bool mis_stop(const MisArgs &a, int idx, int v, unsig
 // already seen out (through L1: a stale "undecided" only costs a redundant store) is
 // skipped. In the first push round nothing is out yet.
 __device__ __forceinline__ void mis_knock(const MisArgs &a, int u, bool check) {
-    if (!check || scan_state(a.state, u) != kOut) a.state[u] = kOut;
+    if (!check || scan_state(a.state, u) != kOut) a.state[sx(u)] = kOut;
 }
 
 // v joined with a row [r0, r0 + deg) longer than kMisLightRow: list it for the next
@@ -941,14 +946,19 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
             // skipping known outs pays when many joiners share neighbours; with few of them
             // the read before each store only lengthens the chain
             const bool check = r >= 2 && nl + nh >= 4096;
-            for (int i = gtid; i < nl; i += gstride) {
+            // lanes per joiner: 1 when the joiners fill the grid, up to 8 when they are few,
+            // so that a short round's rows are not walked one entry at a time by one thread
+            int lpj = 1;
+            while (lpj < 8 && static_cast<long long>(nl) * lpj * 2 <= gstride) lpj <<= 1;
+            const int sub = gtid & (lpj - 1);
+            for (int i = gtid / lpj; i < nl; i += gstride / lpj) {
                 const int j = __ldcg(a.light + i);
                 const int r0 = __ldg(a.row_ptr + j), r1 = __ldg(a.row_ptr + j + 1);
-                pushed += r1 - r0;
-                for (int e = r0; e < r1; e += 8) {
+                if (sub == 0) pushed += r1 - r0;
+                for (int e = r0 + sub; e < r1; e += 8 * lpj) {
                     int u[8];
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) u[k] = e + k < r1 ? __ldg(col + e + k) : j;
+                    for (int k = 0; k < 8; ++k) u[k] = e + k * lpj < r1 ? __ldg(col + e + k * lpj) : j;
 #pragma unroll
                     for (int k = 0; k < 8; ++k)
                         if (u[k] != j) mis_knock(a, u[k], check);
@@ -1011,11 +1021,11 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                     v = r == 0 ? i : __ldcg(qc + i);
                     const int r0 = __ldg(a.row_ptr + v), r1 = __ldg(a.row_ptr + v + 1);
                     if (r == 0 && r1 == r0) {
-                        state[v] = kIn;
-                    } else if (r == 0 || __ldcg(state + v) == kUndecided) {
+                        state[sx(v)] = kIn;
+                    } else if (r == 0 || __ldcg(state + sx(v)) == kUndecided) {
                         const int p = r == 0 ? r0 - 1 : __ldcg(a.pos + v);
-                        if (r == 0) state[v] = kUndecided;
-                        if (p >= r0 && __ldcg(state + __ldg(col + p)) != kOut) {
+                        if (r == 0) state[sx(v)] = kUndecided;
+                        if (p >= r0 && __ldcg(state + sx(__ldg(col + p))) != kOut) {
                             keep = true;  // its blocker is undecided (or joined: its push comes next)
                         } else {
                             const unsigned pv = __ldg(a.prio + v);
@@ -1043,7 +1053,7 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                                 keep = true;
                                 a.pos[v] = stop;
                             } else if (lim >= r1) {
-                                state[v] = kIn;
+                                state[sx(v)] = kIn;
                                 light = r1 - r0 <= kMisLightRow;
                                 if (!light) mis_list_heavy(a, heavy + s0, v, r0, r1 - r0);
                             } else {  // settled up to lim - 1: a warp goes on
@@ -1090,7 +1100,7 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                     if (stop >= 0) {
                         a.pos[v] = stop;
                     } else if (end) {
-                        state[v] = kIn;
+                        state[sx(v)] = kIn;
                         const int r0 = __ldg(a.row_ptr + v);
                         light = r1 - r0 <= kMisLightRow;
                         if (!light) mis_list_heavy(a, heavy + s0, v, r0, r1 - r0);
@@ -1130,7 +1140,7 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
                         a.pos[v] = spos;
                         qn[atomicAdd(qlen + s1, 1)] = v;
                     } else {
-                        state[v] = kIn;
+                        state[sx(v)] = kIn;
                         const int r0 = __ldg(a.row_ptr + v);
                         if (r1 - r0 <= kMisLightRow)
                             a.light[atomicAdd(nlight + s0, 1)] = v;
@@ -1145,7 +1155,7 @@ __global__ void __launch_bounds__(kBlock) mis_kernel(MisArgs a) {
     }
     long long insz = 0;
     for (int i = gtid; i < m; i += gstride) {
-        const unsigned char s = a.state[i];
+        const unsigned char s = a.state[sx(i)];
         if (a.member_i32)
             a.member_i32[i] = (s == kIn) ? 1 : 0;
         else
@@ -1284,11 +1294,17 @@ cudaError_t noalloc_scratch(void **out) {
 
 size_t traversal_scratch_need(int m) { return trav_scratch_bytes(m); }
 
-size_t mis_scratch_need(int m) { return trav_scratch_bytes(m) + Carver::need({static_cast<size_t>(m)}); }
+// what mis_common reserves: the traversal buffers, the state array, the push-unit owners
+// and the list of light joiners
+size_t mis_scratch_need(int m) {
+    const size_t mi = static_cast<size_t>(m) + 1;
+    return trav_scratch_bytes(m) + Carver::need({static_cast<size_t>(m) * kMisStateStride, mi * 4, mi * 4});
+}
 
 apspie_status trav_reserve(apspie_ctx *ctx, int m) {
     void *base;
-    return scratch_reserve(ctx, trav_scratch_bytes(m) + static_cast<size_t>(m) * 5 + 512, &base);
+    return scratch_reserve(ctx, std::max(trav_scratch_bytes(m) + static_cast<size_t>(m) * 5 + 512, mis_scratch_need(m)),
+                           &base);
 }
 
 }  // namespace apspie
@@ -1510,8 +1526,7 @@ static apspie_status mis_common(apspie_ctx *ctx, const apspie_csr *A, const uint
     void *base;
     const size_t tb = trav_scratch_bytes(A->m);
     const size_t mi = static_cast<size_t>(A->m) + 1;
-    const size_t extra = Carver::need({static_cast<size_t>(A->m), mi * 4, mi * 4});
-    st = scratch_reserve(ctx, tb + extra, &base);
+    st = scratch_reserve(ctx, mis_scratch_need(A->m), &base);
     if (st != APSPIE_OK) return st;
     if ((st = reset_ctl(ctx)) != APSPIE_OK) return st;
     MisArgs a;
@@ -1532,7 +1547,7 @@ static apspie_status mis_common(apspie_ctx *ctx, const apspie_csr *A, const uint
     a.heavy_base = buf.rs;
     a.heavy_delta = buf.loc_off;
     Carver c(static_cast<char *>(base) + tb);
-    a.state = c.take<unsigned char>(A->m);
+    a.state = c.take<unsigned char>(static_cast<size_t>(A->m) * kMisStateStride);
     a.unit_owner = c.take<int>(mi);
     a.light = c.take<int>(mi);
     // push units hold at least 128 entries, and few enough that the units of a round's
