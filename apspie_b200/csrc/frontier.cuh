@@ -1,4 +1,5 @@
-// The frontier expander shared by the persistent BFS / SSSP / MIS kernels.
+// The frontier expander shared by the persistent BFS and SSSP kernels (single-source and
+// batched).
 //
 // It replaces the reference's per-level library chain (src/mXv.cuh:142-176,
 // src/spmspvBfs.cuh:178-186, src/spmspvMis.cuh:245-263): Scan -> streamCompact ->
@@ -27,7 +28,7 @@
 namespace apspie {
 
 // Per-warp staging slice. EXTRA adds the second payload and the per-entry accumulator
-// (MIS, batched SSSP); BFS and SSSP leave them out to keep shared memory (occupancy) down.
+// (batched BFS and SSSP); BFS and SSSP leave them out to keep shared memory (occupancy) down.
 template <int WT, bool EXTRA>
 struct WarpSlice {
     int off[WT + 1];   // global edge offset of each staged entry
